@@ -1,0 +1,198 @@
+/*
+ * sbletkf.h -- C ABI of the B200 (sm_100a) sbPOM-LETKF analysis step.
+ *
+ * This library replaces the analysis step of sbPOM-LETKF v2: the per-grid-point
+ * local ensemble transform (LETKF) and the local particle filter (LPF / LPFGM).
+ * Every entry point takes plain pointers and sizes, returns an int status and
+ * never synchronises the stream unless its comment says so.  All array
+ * arguments are DEVICE pointers unless marked "host".
+ *
+ * Array layouts follow the reference's Fortran column-major arrays, written
+ * here as C index order [slowest]...[fastest]:
+ *   fcst3d(nij1,nlev,nmem,nv3d)  ->  [nv3d][nmem][nlev][nij1]
+ *   fcst2d(nij1,nmem,nv2d)       ->  [nv2d][nmem][nij1]
+ *   depth1(nij1,nlev)            ->  [nlev][nij1]
+ *   obshdxf(nobs,nmem)           ->  [nmem][nobs]
+ * Grid point p of the analysis loop (common_da.f90:67-68, DO k / DO i) is
+ * p = (k-1)*nij1 + (i-1).
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   da_main(fcst3d,fcst2d,anal3d,anal2d)      letkf/run/src/common_da.f90:22
+ *   letkf_core(nobsl,hdxf,rdiag,rloc,dep,..)  letkf/run/src/common_letkf.f90:61
+ *   letkf_core_noobs(wvec,Wmat)               letkf/run/src/common_letkf.f90:37
+ *   lpfgm_core(nobsl,hdxf,rdiag,rloc,dep,..)  letkf/run/src/common_lpfgm.f90:444
+ *   lpfgm_core_noobs(wvec,Wmat)               letkf/run/src/common_lpfgm.f90:422
+ *   obs sort / nobsgrd                        letkf/run/src/common_obs.f90:266-377
+ *   compile-time PARAMETERs                   letkf/run/src/common_setting.f90:15-131
+ */
+#ifndef SBLETKF_H
+#define SBLETKF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SBLETKF_ABI_VERSION 1
+
+/* ---- status codes (bit flags; several may be OR-ed together) ---------- */
+#define SBLETKF_OK              0
+#define SBLETKF_ERR_ARG         1   /* bad pointer, shape or parameter          */
+#define SBLETKF_ERR_CUDA        2   /* CUDA runtime error                       */
+#define SBLETKF_ERR_WORKSPACE   4   /* call exceeds the workspace's capacity    */
+#define SBLETKF_ERR_OBS_CELL    8   /* obs cell index outside [1,nlon-1]x[1,nlat-1] */
+#define SBLETKF_ERR_EIG_NOCONV  16  /* Jacobi reached its sweep cap             */
+#define SBLETKF_ERR_NONFINITE   32  /* NaN/Inf met in inputs or in the transform */
+#define SBLETKF_ERR_EIG_NEG     64  /* all eigenvalues negative (common.f90:1031) */
+#define SBLETKF_ERR_ROWS        128 /* local search box has too many grid rows  */
+#define SBLETKF_ERR_UNSUPPORTED 256 /* option not supported by this entry point */
+
+/* ---- enumerations ----------------------------------------------------- */
+#define SBLETKF_F32 0               /* dtype codes */
+#define SBLETKF_F64 1
+
+#define SBLETKF_PREC_FP64  0        /* every step in FP64 (plain path)          */
+#define SBLETKF_PREC_MIXED 1        /* Gram on tcgen05 BF16 hi/lo split, FP32
+                                       accumulate; eigensolve and transform FP64 */
+
+#define SBLETKF_DA_LETKF 1          /* iswitch_da (common_setting.f90:65) */
+#define SBLETKF_DA_LPF   2
+#define SBLETKF_DA_LPFGM 3
+
+#define SBLETKF_RM_SR 0             /* RM (common_setting.f90:82) */
+#define SBLETKF_RM_MR 1
+
+/* ---- run-time parameters (common_setting.f90 PARAMETERs) --------------- */
+typedef struct sbletkf_params {
+  int32_t nmem;        /* ensemble size k            (common_setting.f90:36)  */
+  int32_t nlon, nlat;  /* global grid                 (:37-38)                */
+  int32_t nlev;        /* sigma levels, k=nlev is the surface (:39)          */
+  int32_t nv3d, nv2d;  /* number of 3D / 2D variables (:40-41)               */
+  int32_t iv3d_t;      /* 0-based index of temperature among 3D vars (:44)   */
+  int32_t iv3d_s;      /* 0-based index of salinity (:45)                    */
+  int32_t iswitch_da;  /* SBLETKF_DA_*                (:65)                   */
+  int32_t nmonte;      /* LPF resamplings averaged    (:79)                   */
+  int32_t rm;          /* SBLETKF_RM_SR / _MR         (:82)                   */
+  int32_t dp;          /* diagonal priority on/off    (:85)                   */
+  int32_t sr_textbook; /* 0: reference SR offsets (common_lpfgm.f90:115-117),
+                          1: textbook (u+i-1)/k                               */
+  int32_t roff;        /* T/S round-off on/off        (:129)                  */
+  int32_t id_z_obs;    /* SSH element id              (:59)                   */
+  int32_t precision;   /* SBLETKF_PREC_*                                      */
+  int32_t max_sweeps;  /* Jacobi sweep cap (status flag when reached)         */
+  int32_t reserved_i[3];
+  double cov_infl_mul; /* multiplicative inflation rho (:71)                  */
+  double cov_infl_gm;  /* LPFGM inflation            (:89)                    */
+  double alpha_rtpp;   /* (:74)                                               */
+  double alpha_rtps;   /* (:75)                                               */
+  double sigma_obs;    /* horizontal localization scale [m] (:94)             */
+  double sigma_obsv;   /* vertical scale [m]; <=0 disables it (:95)           */
+  double dist_zero;    /* horizontal cutoff [m]      (:97)                    */
+  double dist_zerov;   /* vertical cutoff [m]        (:98)                    */
+  double tmin, tmax;   /* T round-off bounds         (:130)                   */
+  double smin, smax;   /* S round-off bounds         (:131)                   */
+  double re;           /* earth radius [m]           (:28)                    */
+  double pi;           /* (:27)                                               */
+  double jacobi_tol;   /* relative off-diagonal tolerance of the eigensolve   */
+  double reserved_d[3];
+} sbletkf_params;
+
+/* Local grid of the points analysed (set_common_mpi_pom, common_pom.f90:125-219) */
+typedef struct sbletkf_grid {
+  int32_t nij1;                     /* horizontal points                      */
+  int32_t reserved;
+  const double *lon1, *lat1;        /* [nij1] degrees                         */
+  const double *ri1, *rj1;          /* [nij1] 1-based grid indices            */
+  const double *dlon1, *dlat1;      /* [nij1] grid spacing [m]                */
+  const double *phi1;               /* [nij1] bottom depth h (1 on land)      */
+  const double *depth1;             /* [nlev][nij1] depth [m], <=0            */
+} sbletkf_grid;
+
+/* Observations after H(x) (module globals of common_setting.f90:182-198)     */
+typedef struct sbletkf_obs {
+  int32_t nobs;
+  int32_t hdxf_dtype;               /* SBLETKF_F32 or SBLETKF_F64             */
+  const int32_t *elm;               /* [nobs] element id                      */
+  const int32_t *idx, *idy;         /* [nobs] 1-based owning cell (obs_id_uniform) */
+  const double *lon, *lat;          /* [nobs] degrees                         */
+  const double *lev;                /* [nobs] depth [m], 0 at the surface     */
+  const double *err;                /* [nobs] obs error std; rdiag = err^2    */
+  const double *dep;                /* [nobs] innovation y - H(xf mean)       */
+  const void *hdxf;                 /* [nmem][nobs] dYf = H(dXf)              */
+} sbletkf_obs;
+
+typedef struct sbletkf_workspace sbletkf_workspace;
+
+/* Library ABI version and build information (host). */
+int32_t sbletkf_abi_version(void);
+
+/* Create a workspace on `device` for nij1 points and up to max_nobs
+ * observations.  Allocates all device memory the other entry points use.
+ * No reference counterpart (the reference uses module globals). */
+int sbletkf_workspace_create(const sbletkf_params *p, int32_t nij1, int32_t max_nobs,
+                             int32_t device, sbletkf_workspace **out);
+int sbletkf_workspace_destroy(sbletkf_workspace *ws);
+
+/* Bucket the observations by owning cell, row-major (idy, then idx, stable
+ * within a cell), build the cumulative cell counts (nobsgrd) and the internal
+ * sorted copies of the obs arrays.  Replaces common_obs.f90:266-377. */
+int sbletkf_prepare_obs(sbletkf_workspace *ws, const sbletkf_params *p,
+                        const sbletkf_obs *obs, void *stream);
+
+/* The analysis step: da_main (common_da.f90:22-124) for every point of the
+ * grid, LETKF / LPF / LPFGM by p->iswitch_da, followed by RTPP, RTPS and the
+ * T/S round-off.  fcst3d/anal3d are [nv3d][nmem][nlev][nij1] and
+ * fcst2d/anal2d [nv2d][nmem][nij1], of state_dtype.  uniforms: NULL for LETKF; for LPF/LPFGM
+ * the resampling uniforms, [P][nmonte] (SR) or [P][nmonte][nmem] (MR).
+ * resample_src: optional [P][nmonte][nmem] int32, the particle (0-based)
+ * taken by each member in each draw.  point_status: optional [P] int32.
+ * Asynchronous: errors are latched in the workspace (sbletkf_get_status). */
+int sbletkf_analysis(sbletkf_workspace *ws, const sbletkf_params *p,
+                     const sbletkf_grid *grid,
+                     const void *fcst3d, const void *fcst2d,
+                     void *anal3d, void *anal2d, int32_t state_dtype,
+                     const double *uniforms, int32_t *resample_src,
+                     int32_t *point_status, void *stream);
+
+/* Per-point nobsl (count_nobsl, common_da.f90:133-205) for every point,
+ * int32 [P].  Asynchronous. */
+int sbletkf_count_nobsl(sbletkf_workspace *ws, const sbletkf_params *p,
+                        const sbletkf_grid *grid, int32_t *nobsl, void *stream);
+
+/* Synchronise `stream`, return and clear the latched device status. */
+int sbletkf_get_status(sbletkf_workspace *ws, void *stream, int32_t *status);
+
+/* Ragged batch of per-point cores: letkf_core / letkf_core_noobs
+ * (common_letkf.f90:37-210) or lpfgm_core / lpfgm_core_noobs
+ * (common_lpfgm.f90:422-494) on npts independent local problems.
+ * off[npts+1] (int64) are the row offsets of each point's local obs; point q's
+ * hdxf is the Fortran array hdxf(nobsl,nmem) at hdxf + off[q]*nmem, i.e.
+ * element (i,m) at off[q]*nmem + m*nobsl_q + i.  rdiag/rloc/dep are [off[npts]].
+ * Outputs wvec [npts][nmem] and Wmat [npts][nmem][nmem], Wmat(i,j) of point q
+ * at q*nmem*nmem + j*nmem + i.  uniforms/resample_src as in sbletkf_analysis
+ * with P = npts.  Uses workspace-free device code; asynchronous. */
+int sbletkf_core_batched(const sbletkf_params *p, int32_t npts, const int64_t *off,
+                         const double *hdxf, const double *rdiag, const double *rloc,
+                         const double *dep, double *wvec, double *wmat,
+                         const double *uniforms, int32_t *resample_src,
+                         int32_t *point_status, void *stream);
+
+/* Vector-Jacobian product of the LETKF analysis (iswitch_da = 1, RTPS = 0):
+ * given dJ/d anal3d and dJ/d anal2d (same layouts as the state, state_dtype),
+ * accumulate dJ/d dep and dJ/d rdiag ([nobs], caller's obs order, FP64,
+ * added to), dJ/d cov_infl_mul and dJ/d sigma_obs (one FP64 each, added to).
+ * dist_zero is held fixed.  Recomputes each point's eigensolve.  No
+ * reference counterpart (new capability). */
+int sbletkf_backward(sbletkf_workspace *ws, const sbletkf_params *p,
+                     const sbletkf_grid *grid,
+                     const void *fcst3d, const void *fcst2d, int32_t state_dtype,
+                     const void *grad_anal3d, const void *grad_anal2d,
+                     double *grad_dep, double *grad_rdiag,
+                     double *grad_infl, double *grad_sigma_obs, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SBLETKF_H */

@@ -1,0 +1,375 @@
+// analysis.cu -- the analysis step, one CTA per grid point (FP64 path).
+//
+// Replaces the body of the (k,i) loop of da_main (letkf/run/src/common_da.f90:
+// 67-116): local observation selection (count_nobsl / obs_local, :133-293) as a
+// single streaming pass over the search box in the reference's candidate order,
+// the LETKF / LPF / LPFGM transform, the ensemble update with RTPP / RTPS, and
+// the T/S round-off (:506-533), which is per point and so fused here.
+//
+// The transform is applied without forming W or Pa:
+//   anal_v = xm_v + dX_v V c  +  (dX_v V) diag(sqrt((k-1)/lambda)) V^T
+// with c = Lambda^-1 V^T b, b = Y^T R^-1 rho dep; this equals
+// xm + dX (wvec 1^T + W) of Analysis_Ensemble (:407-432) up to rounding.
+#include "point.cuh"
+
+namespace sbl {
+namespace {
+
+template <int R, typename ST>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_analysis(const sbletkf_params p, const GridView g, const ObsView ob, const ST *__restrict__ f3,
+               const ST *__restrict__ f2, ST *__restrict__ a3, ST *__restrict__ a2, const double *__restrict__ uni,
+               int32_t *__restrict__ src_out, int32_t *__restrict__ pst, int *status, long long p0) {
+  constexpr int KP = kp_of_r(R);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PointSmem S;
+  const int k = p.nmem;
+  S.carve(smem_raw, k, KP);
+  const int tid = threadIdx.x;
+  const long long pid = p0 + blockIdx.x;
+  const int nij1 = g.nij1, nlev = p.nlev;
+  const int kl = (int)(pid / nij1), i = (int)(pid % nij1);
+  const bool do_pf = p.iswitch_da != SBLETKF_DA_LETKF;
+  const bool do_gram = p.iswitch_da != SBLETKF_DA_LPF;
+  __shared__ int sh[8];
+  __shared__ double shd[4];
+  int bits = 0;
+
+  // ---- search box and its grid rows (common_da.f90:158-161, 314-346)
+  if (tid == 0) {
+    int imin, imax, jmin, jmax;
+    search_box(p, g, i, imin, imax, jmin, jmax);
+    int nrows = jmax - jmin + 1;
+    if (nrows < 0) nrows = 0;
+    if (nrows > kRowMax) {
+      nrows = kRowMax;
+      sh[5] = SBLETKF_ERR_ROWS;
+    } else {
+      sh[5] = 0;
+    }
+    sh[0] = imin; sh[1] = imax; sh[2] = jmin; sh[4] = nrows;
+    shd[0] = g.depth1[pid];
+    shd[1] = g.lon1[i];
+    shd[2] = g.lat1[i];
+    shd[3] = g.phi1[i];
+  }
+  __syncthreads();
+  bits |= sh[5];
+  const int imin = sh[0], imax = sh[1], jmin = sh[2], nrows = sh[4];
+  const double rdep = shd[0], plon = shd[1], plat = shd[2], phi = shd[3];
+  {
+    int lens[4], loc = 0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int r = tid * 4 + t;
+      lens[t] = 0;
+      if (r < nrows) {
+        const int j = jmin + r;
+        const int st = ob.cellstart[(long)(j - 1) * p.nlon + (imin - 1)];
+        const int en = ob.cellstart[(long)(j - 1) * p.nlon + imax];
+        S.rowstart[r] = st;
+        lens[t] = en > st ? en - st : 0;
+        loc += lens[t];
+      }
+    }
+    int excl;
+    const int tot = block_excl_scan(loc, excl, S.iws);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int r = tid * 4 + t;
+      if (r < nrows) {
+        S.rowpref[r] = excl;
+        excl += lens[t];
+      }
+    }
+    if (tid == 0) S.rowpref[nrows] = tot;
+    __syncthreads();
+  }
+  const int ncand = S.rowpref[nrows];
+
+  // ---- streaming local-obs selection + accumulation (obs order preserved)
+  Accum<R> A;
+  A.zero();
+  int L = 0, nacc = 0;
+  for (int base = 0; base < ncand; base += kThreads) {
+    const int c = base + tid;
+    int accept = 0, o = 0;
+    double rl = 0.0;
+    if (c < ncand) {
+      int lo = 0, hi = nrows - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (S.rowpref[mid] <= c) lo = mid;
+        else hi = mid - 1;
+      }
+      o = S.rowstart[lo] + (c - S.rowpref[lo]);
+      const double dl = dlev_of(ob.elm[o], ob.lev[o], rdep, kl, nlev, p.id_z_obs);
+      if (!(p.dist_zerov < dl)) {
+        const double dist = distance_2p(ob.lon[o], ob.lat[o], plon, plat, p.pi, p.re);
+        if (!(p.dist_zero < dist)) {
+          accept = 1;
+          rl = loc_weight(dist, dl, p.sigma_obs, p.sigma_obsv);
+        }
+      }
+    }
+    int excl;
+    const int tot = block_excl_scan(accept, excl, S.iws);
+    if (accept) {
+      const int q = L + excl;
+      const double rd = ob.rdiag[o], dp = ob.dep[o];
+      S.lidx[q] = o;
+      S.lrloc[q] = rl;
+      S.lrdiag[q] = rd;
+      S.ldep[q] = dp;
+      const double w = rl / rd;
+      S.lw[q] = w;
+      S.lwd[q] = w * dp;
+    }
+    L += tot;
+    nacc += tot;
+    __syncthreads();
+    int f = 0;
+    while (L - f >= kChunk) {
+      constexpr int KP2 = KP / 2;
+      for (int e = tid; e < kChunk * KP2; e += kThreads) {
+        const int cc = e / KP2, col = e - cc * KP2;
+        reinterpret_cast<double2 *>(S.u)[e] =
+            reinterpret_cast<const double2 *>(ob.hdxf64 + (long)S.lidx[f + cc] * ob.ldh)[col];
+      }
+      __syncthreads();
+      accumulate_chunk<R>(S, f, kChunk, k, do_gram, do_pf, A);
+      f += kChunk;
+    }
+    const int rem = L - f;
+    if (f > 0 && rem > 0) {
+      if (tid < rem) {
+        const int s = f + tid;
+        S.lidx[tid] = S.lidx[s];
+        S.lrloc[tid] = S.lrloc[s];
+        S.lrdiag[tid] = S.lrdiag[s];
+        S.ldep[tid] = S.ldep[s];
+        S.lw[tid] = S.lw[s];
+        S.lwd[tid] = S.lwd[s];
+      }
+      __syncthreads();
+    }
+    L = rem;
+  }
+  if (L > 0) {
+    constexpr int KP2 = KP / 2;
+    for (int e = tid; e < L * KP2; e += kThreads) {
+      const int cc = e / KP2, col = e - cc * KP2;
+      reinterpret_cast<double2 *>(S.u)[e] =
+          reinterpret_cast<const double2 *>(ob.hdxf64 + (long)S.lidx[cc] * ob.ldh)[col];
+    }
+    __syncthreads();
+    accumulate_chunk<R>(S, 0, L, k, do_gram, do_pf, A);
+  }
+
+  // ---- transform
+  const bool surf = (kl == nlev - 1);
+  const int nvt = p.nv3d + (surf ? p.nv2d : 0);
+  if (nacc > 0 && do_gram) {
+    const double alpha = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
+    store_gram<R>(S, k, alpha, A);
+    const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
+    bits |= jacobi_eig(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40);
+    if (tid < k) {  // c = Lambda^-1 V^T b
+      const double *vj = S.u + (long)tid * S.ldb;
+      double s = 0.0;
+      for (int m = 0; m < k; ++m) s = fma(vj[m], S.b[m], s);
+      S.c[tid] = s / S.lam[tid];
+    }
+  }
+  if (do_pf && tid < k) S.ll[tid] = A.ll;
+
+  // ---- forecast block: x, mean, spread, perturbation
+  for (int e = tid; e < nvt * k; e += kThreads) {
+    const int v = e / k, m = e - v * k;
+    double xv;
+    if (v < p.nv3d) xv = (double)f3[(((long)v * k + m) * nlev + kl) * nij1 + i];
+    else xv = (double)f2[((long)(v - p.nv3d) * k + m) * nij1 + i];
+    S.x[v * KP + m] = xv;
+  }
+  __syncthreads();
+  mean_spread_pert(S, KP, k, nvt);
+
+  const double *B = S.u;
+  if (nacc > 0 && do_gram) {
+    // T = dX V
+    for (int e = tid; e < nvt * k; e += kThreads) {
+      const int v = e / k, j = e - v * k;
+      const double *vj = B + (long)j * S.ldb;
+      const double *xv = S.x + v * KP;
+      double s = 0.0;
+      for (int m = 0; m < k; ++m) s = fma(xv[m], vj[m], s);
+      S.t[v * KP + j] = s;
+    }
+    __syncthreads();
+    {  // mean increment dX wvec = T c (LETKF), or dX w_gm (LPFGM)
+      const int lane = tid & 31, wid = tid >> 5;
+      for (int v = wid; v < nvt; v += kThreads / 32) {
+        double s = 0.0;
+        for (int j = lane; j < k; j += 32) s = fma(S.t[v * KP + j], S.c[j], s);
+        s = __shfl_sync(0xffffffffu, warp_sum(s), 0);
+        if (lane == 0) S.misc[16 + v] = s;
+      }
+    }
+    __syncthreads();
+    const bool letkf = p.iswitch_da == SBLETKF_DA_LETKF;
+    for (int e = tid; e < nvt * k; e += kThreads) {
+      const int v = e / k, j = e - v * k;
+      const double lj = S.lam[j];
+      S.t[v * KP + j] *= letkf ? sqrt((double)(k - 1) / lj) : 1.0 / lj;
+    }
+    __syncthreads();
+    // LETKF: anal = xm + dX wvec + T2 V^T
+    // LPFGM: U = dX W_GM = (dX w) 1^T + alpha dX Pa  (W_GM = w 1^T + alpha Pa,
+    //        equal to I + Pa (R^-1 Y)^T (dep 1^T - Y) of gm_core, common_lpfgm.f90:384-397)
+    const double agm = (double)(k - 1) / p.cov_infl_gm;
+    double *dst = letkf ? S.an : S.w;
+    for (int e = tid; e < nvt * k; e += kThreads) {
+      const int v = e / k, m = e - v * k;
+      const double *tv = S.t + v * KP;
+      double s = 0.0;
+      for (int j = 0; j < k; ++j) s = fma(tv[j], B[(long)j * S.ldb + m], s);
+      dst[v * KP + m] = letkf ? S.misc[v] + S.misc[16 + v] + s : S.misc[16 + v] + agm * s;
+    }
+    __syncthreads();
+  } else if (!do_pf || nacc == 0) {
+    // letkf_core_noobs: W = sqrt(rho) I ; lpfgm_core_noobs: W = I
+    const double d = (p.iswitch_da == SBLETKF_DA_LETKF) ? sqrt(p.cov_infl_mul) : 1.0;
+    for (int e = tid; e < nvt * k; e += kThreads) {
+      const int v = e / k, m = e - v * k;
+      S.an[v * KP + m] = S.misc[v] + S.x[v * KP + m] * d;
+    }
+    __syncthreads();
+  }
+
+  if (do_pf && nacc > 0) {
+    // LPF weights and nmonte resamplings; anal_j = xm + mean_d U[src_d(j)]
+    pf_weights(S, k);
+    const double *U = (p.iswitch_da == SBLETKF_DA_LPF) ? S.x : S.w;
+    int16_t *srcb = reinterpret_cast<int16_t *>(S.u);
+    uint8_t *hist = reinterpret_cast<uint8_t *>(srcb + kDrawBatch * k);
+    for (int e = tid; e < nvt * k; e += kThreads) S.an[(e / k) * KP + e % k] = 0.0;
+    for (int d0 = 0; d0 < p.nmonte; d0 += kDrawBatch) {
+      const int nb = min(kDrawBatch, p.nmonte - d0);
+      __syncthreads();
+      if (tid < nb) {
+        const int d = d0 + tid;
+        const double *u = (p.rm == SBLETKF_RM_SR) ? uni + pid * p.nmonte + d : uni + (pid * p.nmonte + d) * k;
+        int16_t *sr = srcb + tid * k;
+        resample_draw(p, S.cw, k, u, hist + tid * k, sr);
+        if (src_out) {
+          int32_t *so = src_out + (pid * p.nmonte + d) * k;
+          for (int j = 0; j < k; ++j) so[j] = sr[j];
+        }
+      }
+      __syncthreads();
+      for (int e = tid; e < nvt * k; e += kThreads) {
+        const int v = e / k, j = e - v * k;
+        double s = S.an[v * KP + j];
+        for (int t = 0; t < nb; ++t) s += U[v * KP + srcb[t * k + j]];
+        S.an[v * KP + j] = s;
+      }
+    }
+    __syncthreads();
+    const double inv = 1.0 / (double)p.nmonte;
+    for (int e = tid; e < nvt * k; e += kThreads) {
+      const int v = e / k, j = e - v * k;
+      S.an[v * KP + j] = S.misc[v] + S.an[v * KP + j] * inv;
+    }
+    __syncthreads();
+  }
+
+  // ---- RTPP / RTPS / round-off, then store
+  relax_and_clamp(p, S, KP, k, nvt, kl, phi);
+  for (int e = tid; e < nvt * k; e += kThreads) {
+    const int v = e / k, m = e - v * k;
+    const double a = S.an[v * KP + m];
+    if (v < p.nv3d) a3[(((long)v * k + m) * nlev + kl) * nij1 + i] = (ST)a;
+    else a2[((long)(v - p.nv3d) * k + m) * nij1 + i] = (ST)a;
+  }
+  if (tid == 0) {
+    if (pst) pst[pid] = bits;
+    if (bits) atomicOr(status, bits);
+  }
+}
+
+// count_nobsl (common_da.f90:133-205): one warp per point.
+__global__ void k_count(const sbletkf_params p, const GridView g, const ObsView ob, int32_t *__restrict__ nobsl,
+                        long long npts, int *status) {
+  const int lane = threadIdx.x & 31;
+  const long long pid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (pid >= npts) return;
+  const int nij1 = g.nij1;
+  const int kl = (int)(pid / nij1), i = (int)(pid % nij1);
+  int imin, imax, jmin, jmax;
+  search_box(p, g, i, imin, imax, jmin, jmax);
+  const double rdep = g.depth1[pid], plon = g.lon1[i], plat = g.lat1[i];
+  int cnt = 0;
+  for (int j = jmin; j <= jmax; ++j) {
+    const int st = ob.cellstart[(long)(j - 1) * p.nlon + (imin - 1)];
+    const int en = ob.cellstart[(long)(j - 1) * p.nlon + imax];
+    for (int o = st + lane; o < en; o += 32) {
+      const double dl = dlev_of(ob.elm[o], ob.lev[o], rdep, kl, p.nlev, p.id_z_obs);
+      if (p.dist_zerov < dl) continue;
+      const double dist = distance_2p(ob.lon[o], ob.lat[o], plon, plat, p.pi, p.re);
+      if (p.dist_zero < dist) continue;
+      ++cnt;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0) nobsl[pid] = cnt;
+  (void)status;
+}
+
+template <int R, typename ST>
+int launch_r(const sbletkf_params *p, const GridView &g, const ObsView &ob, const void *f3, const void *f2, void *a3,
+             void *a2, const double *uni, int32_t *src, int32_t *pst, int *status, cudaStream_t s) {
+  const size_t smem = PointSmem::bytes(p->nmem, kp_of_r(R));
+  auto kern = k_analysis<R, ST>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_status(e);
+  const long long P = (long long)p->nlev * g.nij1;
+  const long long maxg = 2147483647LL;
+  for (long long p0 = 0; p0 < P; p0 += maxg) {
+    const long long n = P - p0 < maxg ? P - p0 : maxg;
+    kern<<<(unsigned)n, kThreads, smem, s>>>(*p, g, ob, (const ST *)f3, (const ST *)f2, (ST *)a3, (ST *)a2, uni,
+                                              src, pst, status, p0);
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+template <typename ST>
+int launch_t(const sbletkf_params *p, const GridView &g, const ObsView &ob, const void *f3, const void *f2, void *a3,
+             void *a2, const double *uni, int32_t *src, int32_t *pst, int *status, cudaStream_t s) {
+  switch (r_for_k(p->nmem)) {
+    case 2: return launch_r<2, ST>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+    case 4: return launch_r<4, ST>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+    case 7: return launch_r<7, ST>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+    default: return launch_r<8, ST>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+  }
+}
+
+}  // namespace
+
+int launch_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, const void *f3,
+                    const void *f2, void *a3, void *a2, int dtype, const double *uni, int32_t *src, int32_t *pst,
+                    cudaStream_t s) {
+  const ObsView ob = ws->obs_view();
+  if (dtype == SBLETKF_F64) return launch_t<double>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, s);
+  return launch_t<float>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, s);
+}
+
+int launch_count(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, int32_t *nobsl,
+                 cudaStream_t s) {
+  const ObsView ob = ws->obs_view();
+  const long long P = (long long)p->nlev * g.nij1;
+  const int wpb = 8;
+  k_count<<<(unsigned)((P + wpb - 1) / wpb), wpb * 32, 0, s>>>(*p, g, ob, nobsl, P, ws->d_status);
+  return cuda_status(cudaGetLastError());
+}
+
+}  // namespace sbl

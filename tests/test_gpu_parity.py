@@ -1,0 +1,141 @@
+"""GPU parity of the analysis step against the FP64 oracle (through the C ABI).
+
+Tolerances: FP64 path <= 1e-10 relative (max error over a field / max of the
+field, and the same for the analysis increment); PF resampling indices
+bit-exact; float32 state output within float32 rounding (2e-6)."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import cref
+from sbpom_letkf_v2_b200.analysis import Analysis, core_batched
+from sbpom_letkf_v2_b200.params import DA_LETKF, DA_LPF, DA_LPFGM, RM_MR, RM_SR
+from sbpom_letkf_v2_b200.synthetic import WORKLOADS, make_case, pf_uniforms
+from tests._util import GOLDEN_CASES, field_relerr, incr_relerr, load_golden
+
+pytestmark = pytest.mark.gpu
+TOL64 = 1e-10
+
+
+def run_gpu(p, grid, obs, f3, f2, uni=None, dtype=torch.float64, want_src=False, dev="cuda:0"):
+    t = lambda a, dt=None: torch.as_tensor(np.asarray(a), device=dev, dtype=dt)
+    nij1 = grid["lon1"].size
+    an = Analysis(p, nij1, max(1, obs["elm"].size), device=dev)
+    an.prepare_obs({k: t(v) for k, v in obs.items()})
+    g = {k: t(v, torch.float64) for k, v in grid.items()}
+    src = None
+    if want_src:
+        src = torch.full((p.nlev * nij1, p.nmonte, p.nmem), -1, dtype=torch.int32, device=dev)
+    st = torch.zeros(p.nlev * nij1, dtype=torch.int32, device=dev)
+    a3, a2 = an.da_main(g, t(f3, dtype), t(f2, dtype), uniforms=None if uni is None else t(uni, torch.float64),
+                        resample_src=src, point_status=st)
+    nobsl = an.count_nobsl(g).cpu().numpy()
+    out = dict(anal3d=a3.cpu().numpy(), anal2d=a2.cpu().numpy(), nobsl=nobsl, status=st.cpu().numpy(),
+               src=None if src is None else src.cpu().numpy())
+    an.close()
+    return out
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_golden_fixture(name, cuda):
+    d = load_golden(name)
+    p = d["params"]
+    r = run_gpu(p, d["grid"], d["obs"], d["fcst3d"], d["fcst2d"], d.get("uniforms"), want_src="src" in d)
+    assert (r["status"] == 0).all()
+    assert np.array_equal(r["nobsl"], d["nobsl"])
+    assert field_relerr(r["anal3d"], d["anal3d"]) <= TOL64
+    assert field_relerr(r["anal2d"], d["anal2d"]) <= TOL64
+    assert incr_relerr(r["anal3d"], d["anal3d"], d["fcst3d"]) <= TOL64
+    if "src" in d:
+        got = r["src"][d["src_points"]]
+        assert np.array_equal(got, d["src"].astype(np.int32))
+
+
+def _case(k, **kw):
+    wl = WORKLOADS[0].scaled(nlon=24, nlat=18, nlev=6, nmem=k, n_sst=500, n_ssh=150, n_prof=5, seed=300 + k)
+    return make_case(wl, **kw)
+
+
+def _np(case):
+    return ({k: v.numpy() for k, v in case.grid.items()}, {k: v.numpy() for k, v in case.obs.items()},
+            case.fcst3d.numpy(), case.fcst2d.numpy())
+
+
+@pytest.mark.parametrize("k", [5, 20, 33, 50, 64, 100, 128])
+def test_letkf_fp64_vs_c_oracle(k, cuda):
+    case = _case(k, cov_infl_mul=1.1, alpha_rtpp=0.5)
+    g, ob, f3, f2 = _np(case)
+    ref = cref.da_main(case.params, g, ob, f3, f2, rsize=8)
+    r = run_gpu(case.params, g, ob, f3, f2)
+    assert (r["status"] == 0).all()
+    assert np.array_equal(r["nobsl"], ref["nobsl"])
+    assert field_relerr(r["anal3d"], ref["anal3d"]) <= TOL64
+    assert field_relerr(r["anal2d"], ref["anal2d"]) <= TOL64
+    assert incr_relerr(r["anal3d"], ref["anal3d"], f3) <= TOL64
+
+
+@pytest.mark.parametrize("da,rm", [(DA_LPF, RM_SR), (DA_LPF, RM_MR), (DA_LPFGM, RM_SR)])
+def test_pf_indices_bit_exact(da, rm, cuda):
+    case = _case(32, iswitch_da=da, rm=rm, nmonte=5)
+    g, ob, f3, f2 = _np(case)
+    P = case.params.nlev * case.nij1
+    uni = pf_uniforms(P, 5, 32, rm).numpy()
+    ref = cref.da_main(case.params, g, ob, f3, f2, uniforms=uni, rsize=8, want_src=True)
+    r = run_gpu(case.params, g, ob, f3, f2, uni=uni, want_src=True)
+    has = ref["nobsl"].reshape(-1) > 0
+    assert np.array_equal(r["src"][has], ref["src"][has])
+    assert field_relerr(r["anal3d"], ref["anal3d"]) <= TOL64
+
+
+def test_float32_state(cuda):
+    case = _case(20, cov_infl_mul=1.1)
+    g, ob, f3, f2 = _np(case)
+    ref = cref.da_main(case.params, g, ob, f3, f2, rsize=8)
+    r = run_gpu(case.params, g, ob, f3, f2, dtype=torch.float32)
+    assert r["anal3d"].dtype == np.float32
+    assert field_relerr(r["anal3d"], ref["anal3d"]) <= 2e-6
+
+
+def test_no_observations_copies_forecast(cuda):
+    case = _case(8)
+    g, ob, f3, f2 = _np(case)
+    empty = {k: v[..., :0] for k, v in ob.items()}
+    r = run_gpu(case.params, g, empty, f3, f2)
+    assert np.array_equal(r["anal3d"], f3.astype(np.float64))
+    assert np.array_equal(r["anal2d"], f2.astype(np.float64))
+
+
+def test_core_batched_matches_oracle_core(cuda):
+    from oracle import letkf_oracle as O
+    case = _case(20, cov_infl_mul=1.1)
+    p = case.params
+    g, ob, f3, f2 = _np(case)
+    so = O.sort_obs(ob, p.nlon, p.nlat)
+    blocks, pts = [], [(k, i) for k in range(p.nlev) for i in range(0, case.nij1, 29)]
+    for (k, i) in pts:
+        cand, dist = O.column_candidates(p, g, so, i)
+        sel, h, rd, rl, dp, _, _ = O.obs_local(p, so, cand, dist, k, g["depth1"][k, i])
+        blocks.append((h, rd, rl, dp))
+    dev = "cuda:0"
+    nob = torch.tensor([b[0].shape[0] for b in blocks], dtype=torch.int64, device=dev)
+    hd = torch.tensor(np.concatenate([b[0].T.reshape(-1) for b in blocks]), device=dev)
+    cat = lambda j: torch.tensor(np.concatenate([b[j] for b in blocks]), device=dev)
+    wv, wm = core_batched(p, nob, hd, cat(1), cat(2), cat(3))
+    for q, (h, rd, rl, dp) in enumerate(blocks):
+        if h.shape[0] == 0:
+            ev, em = O.letkf_core_noobs(p)
+        else:
+            ev, em = O.letkf_core(p, h, rd, rl, dp)
+        assert np.abs(wm[q].cpu().numpy().T - em).max() <= TOL64 * np.abs(em).max()
+        assert np.abs(wv[q].cpu().numpy() - ev).max() <= TOL64 * max(1.0, np.abs(ev).max())
+
+
+def test_bad_obs_cell_raises(cuda):
+    from sbpom_letkf_v2_b200._abi import SBLETKFError
+    case = _case(8)
+    g, ob, f3, f2 = _np(case)
+    ob = dict(ob)
+    ob["idx"] = ob["idx"].copy()
+    ob["idx"][3] = case.params.nlon  # a cell outside [1, nlon-1]
+    with pytest.raises(SBLETKFError):
+        run_gpu(case.params, g, ob, f3, f2)
