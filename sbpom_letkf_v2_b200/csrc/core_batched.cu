@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       } else {
         // W = W_GM W_LPF, row by row (W_GM is in W)
-        double *row = S.an;
+        double *row = S.lam;  // free after W_GM; S.x..S.w hold the counts
         for (int r = 0; r < k; ++r) {
           __syncthreads();
           for (int ii = tid; ii < k; ii += kThreads) row[ii] = W[(long long)ii * k + r];

@@ -77,10 +77,11 @@ __device__ __forceinline__ void search_box(const sbletkf_params &p, const GridVi
   long long b = fnint(__dadd_rn(g.ri1[i], __ddiv_rn(dz, g.dlon1[i])));
   long long c = fnint(__dsub_rn(g.rj1[i], __ddiv_rn(dz, g.dlat1[i])));
   long long d = fnint(__dadd_rn(g.rj1[i], __ddiv_rn(dz, g.dlat1[i])));
-  imin = (int)(a > 1 ? a : 1);
-  imax = (int)(b < p.nlon ? b : p.nlon);
-  jmin = (int)(c > 1 ? c : 1);
-  jmax = (int)(d < p.nlat ? d : p.nlat);
+  imin = (int)(a > 1 ? (a < p.nlon ? a : p.nlon) : 1);
+  imax = (int)(b < p.nlon ? (b > 1 ? b : 1) : p.nlon);
+  jmin = (int)(c > 1 ? (c < p.nlat ? c : p.nlat) : 1);
+  jmax = (int)(d < p.nlat ? (d > 1 ? d : 1) : p.nlat);
+  // every index is now inside the grid; an empty box has imin > imax or jmin > jmax
 }
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -293,7 +293,7 @@ __device__ __forceinline__ void resample_draw(const sbletkf_params &p, const dou
       if (hist[i]) src[i] = (int16_t)i;
     for (int i = 0; i < k; ++i)
       for (int c = 1; c < hist[i]; ++c) {
-        while (hist[f]) ++f;
+        while (f < k - 1 && hist[f]) ++f;
         src[f++] = (int16_t)i;
       }
   } else {
