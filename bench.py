@@ -1,0 +1,359 @@
+"""Benchmark of the analysis step: gridpoints/s of one LETKF cycle.
+
+Workload (default): 400 x 300 x 40 grid, k = 100 members, 200k observations
+(150k SST, 45k SSH, 500 T/S profiles x 10 levels), sigma_h = 200 km,
+sigma_v = 100 m, rho = 1.1 -- seeded synthetic inputs generated in device
+memory (sbpom_letkf_v2_b200.synthetic).  One step = one analysis cycle:
+observation bucketing (sbletkf_prepare_obs) + the analysis of all 4.8M grid
+points (sbletkf_analysis).  Inputs (7.7 GB of state) exceed L2, so no flush
+is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference      # the CPU restatement on the host cores
+
+Multi-GPU (torchrun): every rank analyses its own copy of the workload
+(independent domains, no collective on the data path) -> weak scaling.
+"""
+from __future__ import annotations
+
+import os
+
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
+import argparse  # noqa: E402
+import json  # noqa: E402
+import statistics  # noqa: E402
+import subprocess  # noqa: E402
+import threading  # noqa: E402
+import time  # noqa: E402
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+METRIC = "analysis gridpoints/s per LETKF cycle, mixed vs FP64 on B200 at <=1e-4 rel err"
+
+
+def _peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def _fp64_peak(dev) -> dict:
+    """FP64 roofline denominator: cuBLAS DGEMM 8192^3 through torch.matmul,
+    best of 5 (the FP64 counterpart of the driver's bf16 GEMM peak)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return {"tflops": 2.0 * n ** 3 / (best / 1e3) / 1e12,
+            "source": "measured: cuBLAS DGEMM 8192^3 via torch.matmul, best of 5"}
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        load = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[j] for r in self.rows for j in range(4) if r[5 + j].lower() == "active"})
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def algorithmic_flops(nobsl: np.ndarray, k: int, nv3d: int, nv2d: int, nlev: int, nij1: int) -> dict:
+    """Per-launch algorithmic work of the analysis (per point with n local obs):
+    F_gram = 2 k^2 n, F_eig = 9 k^3, F_W = 2k^3 + 2kn + 2k^2, F_upd = 2 nv k^2."""
+    n = nobsl.astype(np.float64).reshape(nlev, nij1)
+    has = n > 0
+    nv = np.full_like(n, nv3d, dtype=np.float64)
+    nv[nlev - 1, :] += nv2d
+    f_gram = float((2.0 * k * k * n).sum())
+    f_eig = float((9.0 * k ** 3) * has.sum())
+    f_w = float(((2.0 * k ** 3 + 2.0 * k * n + 2.0 * k * k) * has).sum())
+    f_upd = float((2.0 * nv * k * k).sum())
+    return {"gram": f_gram, "eig": f_eig, "w": f_w, "upd": f_upd, "total": f_gram + f_eig + f_w + f_upd}
+
+
+def cpu_baseline(case, p, seconds: float = 15.0, nthreads: int = 0):
+    """The C restatement (reference default r_size = binary32 build) on a
+    stratified sample of whole grid columns, all levels; returns gridpoints/s."""
+    from oracle import cref
+    nthreads = nthreads or os.cpu_count()
+    nij1 = case.nij1
+    g_all = {k: v.cpu().numpy() for k, v in case.grid.items()}
+    ob = {k: v.cpu().numpy() for k, v in case.obs.items()}
+    si = cref.SortedInputs(p, ob, 4)
+
+    def run(cols):
+        g = {k: (v[:, cols] if v.ndim == 2 else v[cols]) for k, v in g_all.items()}
+        ct = torch.as_tensor(cols, device=case.fcst3d.device)
+        f3 = case.fcst3d[:, :, :, ct].cpu().numpy()
+        f2 = case.fcst2d[:, :, ct].cpu().numpy()
+        t = time.perf_counter()
+        cref.da_main(p, g, ob, f3, f2, rsize=4, nthreads=nthreads, sorted_inputs=si)
+        return time.perf_counter() - t
+
+    rng = np.random.default_rng(5)
+    cal = np.sort(rng.choice(nij1, size=max(nthreads, 16), replace=False))
+    tc = run(cal)
+    ncol = int(min(nij1, max(nthreads, seconds / max(tc, 1e-3) * cal.size)))
+    stride = max(1, nij1 // ncol)
+    cols = np.arange(0, nij1, stride)[:ncol]
+    dt = run(cols)
+    pts = cols.size * p.nlev
+    return {"value": pts / dt, "unit": "gridpoints/s", "cores": nthreads, "kind": "port",
+            "sample": f"{cols.size} of {nij1} columns (every {stride}th, all {p.nlev} levels = {pts} points), "
+                      f"C/OpenMP restatement, r_size=binary32 (reference default build), {dt:.1f} s"}
+
+
+def reference_arm(args, rank, world):
+    """--impl reference: the CPU restatement timed per step on a bounded sample."""
+    from sbpom_letkf_v2_b200.synthetic import WORKLOADS, make_case
+    if rank != 0:
+        return
+    dev = "cuda:0" if torch.cuda.is_available() else "cpu"
+    wl = WORKLOADS[args.workload]
+    case = make_case(wl, device=dev, seed=wl.seed)
+    p = case.params.replace(precision=0)
+    vals = []
+    for s in range(args.warmup + args.steps):
+        r = cpu_baseline(case, p, seconds=args.ref_seconds)
+        if s >= args.warmup:
+            vals.append(r["value"])
+    v = float(np.mean(vals))
+    line = {"metric": METRIC, "value": v, "unit": "gridpoints/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * wl.npoints / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": wl.name, "points": wl.npoints, "nmem": wl.nmem, "nobs": wl.nobs,
+                       "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": v, "unit": "gridpoints/s", "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": v, "unit": "gridpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", type=int, default=1)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=8.0)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = False
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device(f"cuda:{local}"))
+        pg = True
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        if pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    from sbpom_letkf_v2_b200.analysis import Analysis
+    from sbpom_letkf_v2_b200.params import PREC_FP64, PREC_MIXED
+    from sbpom_letkf_v2_b200.synthetic import WORKLOADS, make_case
+
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    wl = WORKLOADS[args.workload]
+    case = make_case(wl, device=dev, seed=wl.seed + rank)
+    prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
+    p = case.params.replace(precision=prec)
+    nobs = case.obs["elm"].numel()
+    an = Analysis(p, case.nij1, nobs, device=dev)
+    an.prepare_obs(case.obs)
+    nobsl = an.count_nobsl(case.grid).cpu().numpy()
+    a3 = torch.empty_like(case.fcst3d)
+    a2 = torch.empty_like(case.fcst2d)
+    s = torch.cuda.current_stream()
+
+    def step():
+        an.prepare_obs(case.obs)
+        an.da_main(case.grid, case.fcst3d, case.fcst2d, anal3d=a3, anal2d=a2, check=False)
+
+    for _ in range(args.warmup):
+        step()
+    an.raise_status()
+
+    def barrier():
+        if pg:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # ---- device-timed region: K steps, with the analysis kernel timed inside
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(dev.index) as clk:
+        t0.record(s)
+        for i in range(args.steps):
+            an.prepare_obs(case.obs)
+            ev[i][0].record(s)
+            an.da_main(case.grid, case.fcst3d, case.fcst2d, anal3d=a3, anal2d=a2, check=False)
+            ev[i][1].record(s)
+        t1.record(s)
+        torch.cuda.synchronize()
+    barrier()
+    ms = t0.elapsed_time(t1) / args.steps
+    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    an.raise_status()
+    if pg:
+        import torch.distributed as dist
+        tt = torch.tensor([ms, kern_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, kern_ms = float(tt[0]), float(tt[1])
+    P = wl.npoints
+    value = P * world / (ms / 1e3)
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        hobs = {k: v.cpu().pin_memory() for k, v in case.obs.items()}
+        hf3 = case.fcst3d.cpu().pin_memory()
+        hf2 = case.fcst2d.cpu().pin_memory()
+        ha3 = torch.empty_like(hf3).pin_memory()
+        ha2 = torch.empty_like(hf2).pin_memory()
+        d_obs = {k: torch.empty_like(v, device=dev) for k, v in hobs.items()}
+        d3 = torch.empty_like(case.fcst3d)
+        d2 = torch.empty_like(case.fcst2d)
+        h2d = sum(v.numel() * v.element_size() for v in hobs.values()) + hf3.numel() * 4 + hf2.numel() * 4
+        d2h = ha3.numel() * 4 + ha2.numel() * 4
+
+        def e2e_step():
+            for k, v in hobs.items():
+                d_obs[k].copy_(v, non_blocking=True)
+            d3.copy_(hf3, non_blocking=True)
+            d2.copy_(hf2, non_blocking=True)
+            an.prepare_obs(d_obs)
+            an.da_main(case.grid, d3, d2, anal3d=a3, anal2d=a2, check=False)
+            ha3.copy_(a3, non_blocking=True)
+            ha2.copy_(a2, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        ne = max(1, min(args.steps, 3))
+        e0.record(s)
+        for _ in range(ne):
+            e2e_step()
+        e1.record(s)
+        torch.cuda.synchronize()
+        barrier()
+        ems = e0.elapsed_time(e1) / ne
+        if pg:
+            import torch.distributed as dist
+            tt = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt[0])
+        e2e = {"value": P * world / (ems / 1e3), "unit": "gridpoints/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": ems}
+
+    if rank == 0:
+        fl = algorithmic_flops(nobsl, p.nmem, p.nv3d, p.nv2d, p.nlev, case.nij1)
+        f64 = _fp64_peak(dev)
+        achieved = fl["total"] / (kern_ms / 1e3) / 1e12
+        if f64:
+            roof = {"bound": "fp64", "achieved": achieved, "peak": f64["tflops"], "unit": "TFLOP/s",
+                    "frac": achieved / f64["tflops"], "traffic": None, "kernel": "k_analysis",
+                    "peak_source": f64["source"], "kernel_ms": kern_ms, "flops_per_launch": fl}
+        else:
+            roof = {"bound": "fp64", "achieved": achieved, "peak": None, "unit": "TFLOP/s", "frac": None,
+                    "traffic": None, "kernel": "k_analysis", "kernel_ms": kern_ms, "flops_per_launch": fl}
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            cpu = cpu_baseline(case, p.replace(precision=PREC_FP64), seconds=15.0)
+        peaks, src = _peaks()
+        line = {"metric": METRIC, "value": value, "unit": "gridpoints/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if prec == PREC_FP64 else "bf16x2+f64",
+                "data": "synthetic (seeded, generated in device memory)",
+                "config": {"workload": wl.name, "points": P, "nmem": p.nmem, "nobs": nobs,
+                           "precision": args.precision, "nobsl_mean": float(nobsl.mean()),
+                           "nobsl_max": int(nobsl.max()), "l2": "inputs larger than L2 (7.7 GB state)",
+                           "parallelism": f"replicas x{world}"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": 6 * args.steps, "peaks_source": src,
+                "hbm_peak_gbs": peaks.get("hbm_gbs")}
+        print(json.dumps(line), flush=True)
+    an.close()
+    if pg:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -10,6 +10,14 @@
 //   anal_v = xm_v + dX_v V c  +  (dX_v V) diag(sqrt((k-1)/lambda)) V^T
 // with c = Lambda^-1 V^T b, b = Y^T R^-1 rho dep; this equals
 // xm + dX (wvec 1^T + W) of Analysis_Ensemble (:407-432) up to rounding.
+//
+// Points with nobsl < k (at most kDualMax) take the observation-space form of
+// the same transform: with Z = diag(sqrt(rloc/rdiag)) Y (n x k) and
+// N = alpha I_n + Z Z^T = Q Lambda Q^T (alpha = (k-1)/rho),
+//   wvec = Z^T Q Lambda^-1 Q^T d,  d = sqrt(rloc/rdiag) dep
+//   W    = sqrt(k-1) [ alpha^-1/2 I + Z^T Q diag(g) Q^T Z ],
+//   g_j  = -1 / ( sqrt(alpha lambda_j) (sqrt(lambda_j) + sqrt(alpha)) ),
+// exact algebra (push-through identity), so only an n x n eigensolve is needed.
 #include "point.cuh"
 
 namespace sbl {
@@ -87,10 +95,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   const int ncand = S.rowpref[nrows];
 
-  // ---- streaming local-obs selection + accumulation (obs order preserved)
+  // ---- streaming local-obs selection + accumulation (obs order preserved).
+  // Rows are consumed on the fly once nobsl exceeds the dual limit; below it
+  // the list is kept for the observation-space transform.
   Accum<R> A;
   A.zero();
   int L = 0, nacc = 0;
+  const int ndm = do_gram ? PointSmem::dual_max(k) : -1;
+  bool primal = ndm < 0;
   for (int base = 0; base < ncand; base += kThreads) {
     const int c = base + tid;
     int accept = 0, o = 0;
@@ -128,6 +140,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     L += tot;
     nacc += tot;
     __syncthreads();
+    if (!primal && L > ndm) primal = true;
+    if (!primal) continue;
     int f = 0;
     while (L - f >= kChunk) {
       constexpr int KP2 = KP / 2;
@@ -155,7 +169,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     L = rem;
   }
-  if (L > 0) {
+  if (primal && L > 0) {
     constexpr int KP2 = KP / 2;
     for (int e = tid; e < L * KP2; e += kThreads) {
       const int cc = e / KP2, col = e - cc * KP2;
@@ -169,7 +183,56 @@ __global__ void __launch_bounds__(kThreads, 1)
   // ---- transform
   const bool surf = (kl == nlev - 1);
   const int nvt = p.nv3d + (surf ? p.nv2d : 0);
-  if (nacc > 0 && do_gram) {
+  const bool dual = !primal && nacc > 0;
+  const int n = nacc;
+  const int ldz = KP + 1, ldn = n | 1;
+  double *Z = S.u, *Nb = S.u + (long)ndm * ldz;
+  const double alpha_d = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
+  if (dual) {
+    // rows of the n local obs, then (LPFGM) the PF log-likelihood in obs order
+    for (int e = tid; e < n * KP; e += kThreads) {
+      const int o = e / KP, m = e - o * KP;
+      Z[o * ldz + m] = ob.hdxf64[(long)S.lidx[o] * ob.ldh + m];
+    }
+    __syncthreads();
+    if (do_pf && tid < k) {
+      double ll = A.ll;
+      for (int o = 0; o < n; ++o) {
+        double d = __dsub_rn(S.ldep[o], Z[o * ldz + tid]);
+        double q = __dmul_rn(__dmul_rn(0.5, d), d);
+        q = __ddiv_rn(__dmul_rn(q, S.lrloc[o]), S.lrdiag[o]);
+        ll = __dsub_rn(ll, q);
+      }
+      A.ll = ll;
+    }
+    __syncthreads();
+    for (int e = tid; e < n * KP; e += kThreads) {
+      const int o = e / KP, m = e - o * KP;
+      Z[o * ldz + m] *= sqrt(S.lw[o]);
+    }
+    if (tid < n) S.b[tid] = sqrt(S.lw[tid]) * S.ldep[tid];
+    __syncthreads();
+    for (int e = tid; e < n * n; e += kThreads) {  // N = alpha I + Z Z^T
+      const int r = e % n, c = e / n;
+      if (r <= c) {
+        double s = 0.0;
+        for (int m = 0; m < k; ++m) s = fma(Z[r * ldz + m], Z[c * ldz + m], s);
+        if (r == c) s += alpha_d;
+        Nb[(long)c * ldn + r] = s;
+        Nb[(long)r * ldn + c] = s;
+      }
+    }
+    __syncthreads();
+    const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
+    bits |= jacobi_eig(Nb, n, ldn, tol, p.max_sweeps, S.lam, S.iws + 40);
+    if (tid < n) {  // c = Lambda^-1 Q^T d
+      const double *qj = Nb + (long)tid * ldn;
+      double s = 0.0;
+      for (int o = 0; o < n; ++o) s = fma(qj[o], S.b[o], s);
+      S.c[tid] = s / S.lam[tid];
+    }
+  }
+  if (!dual && nacc > 0 && do_gram) {
     const double alpha = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
     store_gram<R>(S, k, alpha, A);
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
@@ -195,7 +258,63 @@ __global__ void __launch_bounds__(kThreads, 1)
   mean_spread_pert(S, KP, k, nvt);
 
   const double *B = S.u;
-  if (nacc > 0 && do_gram) {
+  if (dual) {
+    const bool letkf = p.iswitch_da == SBLETKF_DA_LETKF;
+    for (int e = tid; e < nvt * n; e += kThreads) {  // P = dX Z^T
+      const int v = e / n, o = e - v * n;
+      const double *xv = S.x + v * KP, *zo = Z + o * ldz;
+      double s = 0.0;
+      for (int m = 0; m < k; ++m) s = fma(xv[m], zo[m], s);
+      S.t[v * KP + o] = s;
+    }
+    __syncthreads();
+    for (int e = tid; e < nvt * n; e += kThreads) {  // Pq = P Q
+      const int v = e / n, j = e - v * n;
+      const double *qj = Nb + (long)j * ldn, *pv = S.t + v * KP;
+      double s = 0.0;
+      for (int o = 0; o < n; ++o) s = fma(pv[o], qj[o], s);
+      S.w[v * KP + j] = s;
+    }
+    __syncthreads();
+    {
+      const int lane = tid & 31, wid = tid >> 5;
+      for (int v = wid; v < nvt; v += kThreads / 32) {  // dX wvec = Pq Lambda^-1 Q^T d
+        double s = 0.0;
+        for (int j = lane; j < n; j += 32) s = fma(S.w[v * KP + j], S.c[j], s);
+        s = __shfl_sync(0xffffffffu, warp_sum(s), 0);
+        if (lane == 0) S.misc[16 + v] = s;
+      }
+    }
+    __syncthreads();
+    const double sa = sqrt(alpha_d);
+    for (int e = tid; e < nvt * n; e += kThreads) {
+      const int v = e / n, j = e - v * n;
+      const double lj = S.lam[j];
+      S.w[v * KP + j] *= letkf ? -1.0 / (sqrt(alpha_d * lj) * (sqrt(lj) + sa)) : 1.0 / lj;
+    }
+    __syncthreads();
+    for (int e = tid; e < nvt * n; e += kThreads) {  // Sq = (Pq g) Q^T
+      const int v = e / n, o = e - v * n;
+      const double *wv = S.w + v * KP;
+      double s = 0.0;
+      for (int j = 0; j < n; ++j) s = fma(wv[j], Nb[(long)j * ldn + o], s);
+      S.t[v * KP + o] = s;
+    }
+    __syncthreads();
+    // LETKF: anal = xm + dX wvec + sqrt(k-1) (alpha^-1/2 dX + Sq Z)
+    // LPFGM: U = dX W_GM = (dX w) 1^T + dX - (dX Z^T Q Lambda^-1 Q^T) Z
+    const double sk = sqrt((double)(k - 1)), isa = 1.0 / sa;
+    for (int e = tid; e < nvt * k; e += kThreads) {
+      const int v = e / k, m = e - v * k;
+      const double *tv = S.t + v * KP;
+      double s = 0.0;
+      for (int o = 0; o < n; ++o) s = fma(tv[o], Z[o * ldz + m], s);
+      const double dx = S.x[v * KP + m];
+      if (letkf) S.an[v * KP + m] = S.misc[v] + S.misc[16 + v] + sk * (isa * dx + s);
+      else S.w[v * KP + m] = S.misc[16 + v] + dx - s;
+    }
+    __syncthreads();
+  } else if (nacc > 0 && do_gram) {
     // T = dX V
     for (int e = tid; e < nvt * k; e += kThreads) {
       const int v = e / k, j = e - v * k;

@@ -12,7 +12,8 @@ constexpr int kNvMax = 8;        // nv3d + nv2d limit
 constexpr int kRowMax = 1024;    // grid rows of one local search box
 constexpr int kThreads = 256;    // CTA size of the per-point kernels
 constexpr int kChunk = 32;       // local obs rows staged per Gram step
-constexpr int kListCap = kThreads + kChunk;
+constexpr int kDualMax = 64;     // local obs handled by the observation-space transform
+constexpr int kListCap = kThreads + kDualMax + kChunk;
 
 // Sorted observation arrays owned by the workspace (cell order of
 // common_obs.f90:266-377).  hdxf rows are padded to ldh with zeros.

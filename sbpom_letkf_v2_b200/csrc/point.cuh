@@ -35,12 +35,17 @@ struct PointSmem {
 
   __host__ __device__ static size_t a16(size_t v) { return (v + 15) & ~size_t(15); }
 
-  // Union size: max(chunk rows, k x ldb matrix, draw buffers).
+  // Largest nobsl that takes the observation-space (dual) transform.
+  __host__ __device__ static int dual_max(int k) { return k - 1 < kDualMax ? k - 1 : kDualMax; }
+  // Union size: max(chunk rows, k x ldb matrix, dual Z and N, draw buffers).
   __host__ __device__ static size_t union_bytes(int k, int kp) {
+    const size_t nd = (size_t)dual_max(k);
     size_t chunk = sizeof(double) * kChunk * kp;
     size_t mat = sizeof(double) * (size_t)k * (kp + 1);
+    size_t dual = sizeof(double) * (nd * (kp + 1) + nd * (nd + 1));
     size_t pf = (size_t)kDrawBatch * k * (sizeof(int16_t) + 1) + 16;
     size_t m = chunk > mat ? chunk : mat;
+    m = m > dual ? m : dual;
     return a16(m > pf ? m : pf);
   }
   __host__ __device__ static size_t fixed_bytes(int kp) {
@@ -153,20 +158,28 @@ __device__ __forceinline__ void store_gram(const PointSmem &S, int k, double alp
   __syncthreads();
 }
 
-// One-sided cyclic Jacobi on the SPD matrix in B (k x k, stride ldb).
-// On return B holds the eigenvectors as columns and lam[] the eigenvalues.
-// Returns status bits (uniform over the CTA).
-static __device__ __noinline__ int jacobi_eig(double *B, int k, int ldb, double tol, int maxsw, double *lam, int *flag) {
+// One-sided cyclic Jacobi on the SPD matrix in B (n x n, column-major,
+// stride ldb, n <= 128).  Round-robin ordering: in each of the n2-1 rounds the
+// n2/2 column pairs are disjoint and are processed concurrently, one 8-lane
+// group per pair (4 pairs per warp).  A pair (p,q) is rotated when
+// |b_p.b_q| > tol |b_p||b_q|; the sweep loop ends after a sweep without
+// rotations.  On return B holds the eigenvectors as columns and lam[] the
+// eigenvalues (column norms).  Returns status bits (uniform over the CTA).
+static __device__ __noinline__ int jacobi_eig(double *B, int n, int ldb, double tol, int maxsw, double *lam,
+                                              int *flag) {
+  constexpr int G = 8, E = 16;  // lanes per pair, elements per lane (n <= G*E)
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int n2 = (k + 1) & ~1, m = n2 - 1;
+  const int grp = lane / G, gl = lane % G, lead = grp * G;
+  const int n2 = (n + 1) & ~1, m = n2 - 1, npair = n2 / 2;
   int bits = 0, sweep = 0;
   if (threadIdx.x == 0) flag[1] = 0;
   for (; sweep < maxsw; ++sweep) {
     if (threadIdx.x == 0) *flag = 0;
     __syncthreads();
     for (int rd = 0; rd < m; ++rd) {
-      for (int pi = wid; pi < n2 / 2; pi += nw) {
-        int a, b;
+      for (int base = wid * (32 / G); base < npair; base += nw * (32 / G)) {
+        const int pi = base + grp;
+        int a = 0, b = 0;
         if (pi == 0) {
           a = m;
           b = rd;
@@ -174,34 +187,42 @@ static __device__ __noinline__ int jacobi_eig(double *B, int k, int ldb, double 
           a = (rd + pi) % m;
           b = (rd - pi + m) % m;
         }
-        if (a >= k || b >= k) continue;
-        double *ca = B + (long)a * ldb, *cb = B + (long)b * ldb;
-        double va[4], vb[4], al = 0.0, be = 0.0, ga = 0.0;
+        const bool act = pi < npair && a < n && b < n;
+        double *ca = B + (long)(act ? a : 0) * ldb, *cb = B + (long)(act ? b : 0) * ldb;
+        double va[E], vb[E], al = 0.0, be = 0.0, ga = 0.0;
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int r = lane + 32 * t;
-          va[t] = r < k ? ca[r] : 0.0;
-          vb[t] = r < k ? cb[r] : 0.0;
+        for (int t = 0; t < E; ++t) {
+          const int r = gl + G * t;
+          const bool in = act && r < n;
+          va[t] = in ? ca[r] : 0.0;
+          vb[t] = in ? cb[r] : 0.0;
           al = fma(va[t], va[t], al);
           be = fma(vb[t], vb[t], be);
           ga = fma(va[t], vb[t], ga);
         }
-        al = __shfl_sync(0xffffffffu, warp_sum(al), 0);
-        be = __shfl_sync(0xffffffffu, warp_sum(be), 0);
-        ga = __shfl_sync(0xffffffffu, warp_sum(ga), 0);
-        if (fabs(ga) > tol * sqrt(al * be)) {
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        // one value per group, so every lane of a pair applies the same rotation
+        al = __shfl_sync(0xffffffffu, al, lead);
+        be = __shfl_sync(0xffffffffu, be, lead);
+        ga = __shfl_sync(0xffffffffu, ga, lead);
+        if (act && fabs(ga) > tol * sqrt(al * be)) {
           const double zeta = (be - al) / (2.0 * ga);
           const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
           const double cs = 1.0 / sqrt(1.0 + tt * tt), sn = cs * tt;
 #pragma unroll
-          for (int t = 0; t < 4; ++t) {
-            const int r = lane + 32 * t;
-            if (r < k) {
+          for (int t = 0; t < E; ++t) {
+            const int r = gl + G * t;
+            if (r < n) {
               ca[r] = cs * va[t] - sn * vb[t];
               cb[r] = sn * va[t] + cs * vb[t];
             }
           }
-          if (lane == 0) *flag = 1;
+          if (gl == 0) *flag = 1;
         }
       }
       __syncthreads();
@@ -211,18 +232,18 @@ static __device__ __noinline__ int jacobi_eig(double *B, int k, int ldb, double 
     if (!rot) break;
   }
   if (sweep >= maxsw) bits |= SBLETKF_ERR_EIG_NOCONV;
-  for (int j = wid; j < k; j += nw) {
+  for (int j = wid; j < n; j += nw) {
     double *cj = B + (long)j * ldb;
     double s = 0.0;
-    for (int r = lane; r < k; r += 32) s = fma(cj[r], cj[r], s);
+    for (int r = lane; r < n; r += 32) s = fma(cj[r], cj[r], s);
     s = __shfl_sync(0xffffffffu, warp_sum(s), 0);
     const double l = sqrt(s);
     if (lane == 0) lam[j] = l;
     const double inv = 1.0 / l;
-    for (int r = lane; r < k; r += 32) cj[r] *= inv;
+    for (int r = lane; r < n; r += 32) cj[r] *= inv;
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < k; j += blockDim.x)
+  for (int j = threadIdx.x; j < n; j += blockDim.x)
     if (!(lam[j] > 0.0) || !isfinite(lam[j])) atomicOr(flag + 1, SBLETKF_ERR_NONFINITE);
   __syncthreads();
   bits |= flag[1];
