@@ -179,6 +179,27 @@ int sbletkf_core_batched(const sbletkf_params *p, int32_t npts, const int64_t *o
                          const double *uniforms, int32_t *resample_src,
                          int32_t *point_status, void *stream);
 
+/* Allocation-free analysis for small problems.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc where they run the
+ * analysis -- e.g. a host model whose memory pool already owns the device
+ * (cudaMalloc would synchronise the device or fail) -- this entry point needs
+ * no workspace: obs bucketing and sbletkf_analysis run with every scratch
+ * buffer in one fixed device array of the library (about 13.4 MB, held by every
+ * GPU that loads the library until exit).  It calls no allocating routine.
+ * Limits: obs->nobs <= SBLETKF_NOALLOC_MAX_OBS, nlon*nlat <=
+ * SBLETKF_NOALLOC_MAX_CELLS, nmem <= 128; larger calls return
+ * SBLETKF_ERR_WORKSPACE before launching anything.  Runs on the current
+ * device; the first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised.
+ * FP64 path only; device-side errors are reported in point_status. */
+#define SBLETKF_NOALLOC_MAX_OBS   8192
+#define SBLETKF_NOALLOC_MAX_CELLS 65536
+int sbletkf_analysis_noalloc(const sbletkf_params *p, const sbletkf_grid *grid, const sbletkf_obs *obs,
+                             const void *fcst3d, const void *fcst2d, void *anal3d, void *anal2d,
+                             int32_t state_dtype, const double *uniforms, int32_t *point_status,
+                             void *stream);
+
 /* Vector-Jacobian product of the LETKF analysis (iswitch_da = 1, RTPS = 0):
  * given dJ/d anal3d and dJ/d anal2d (same layouts as the state, state_dtype),
  * accumulate dJ/d dep and dJ/d rdiag ([nobs], caller's obs order, FP64,

@@ -25,7 +25,8 @@ _NAMES = {ERR_ARG: "bad argument", ERR_CUDA: "CUDA error", ERR_WORKSPACE: "works
 #: every symbol include/sbletkf.h declares
 EXPORTS = ("sbletkf_abi_version", "sbletkf_workspace_create", "sbletkf_workspace_destroy",
            "sbletkf_prepare_obs", "sbletkf_analysis", "sbletkf_count_nobsl", "sbletkf_get_status",
-           "sbletkf_core_batched", "sbletkf_backward")
+           "sbletkf_core_batched", "sbletkf_backward", "sbletkf_analysis_noalloc")
+NOALLOC_MAX_OBS, NOALLOC_MAX_CELLS = 8192, 65536
 
 
 class SBLETKFError(RuntimeError):
@@ -70,6 +71,8 @@ def load(path: str = LIB_PATH):
         "sbletkf_core_batched": ([pp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "sbletkf_backward": ([vp, pp, ctypes.POINTER(CGrid), vp, vp, i32, vp, vp, vp, vp, vp, vp, vp],
                              ctypes.c_int),
+        "sbletkf_analysis_noalloc": ([pp, ctypes.POINTER(CGrid), ctypes.POINTER(CObs), vp, vp, vp, vp, i32, vp,
+                                      vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
