@@ -160,13 +160,23 @@ def cpu_baseline(case, p, seconds: float = 15.0, nthreads: int = 0):
                       f"C/OpenMP restatement, r_size=binary32 (reference default build), {dt:.1f} s"}
 
 
+def scaled_workload(wl, s: int):
+    """The workload with nlon, nlat / s and observation counts / s^2."""
+    if s <= 1:
+        return wl
+    q = s * s
+    return wl.scaled(nlon=max(8, wl.nlon // s), nlat=max(8, wl.nlat // s), n_sst=wl.n_sst // q,
+                     n_ssh=wl.n_ssh // q, n_prof=max(1, wl.n_prof // q), n_hf=wl.n_hf // q,
+                     name=wl.name + f" (1/{s} grid)")
+
+
 def reference_arm(args, rank, world):
     """--impl reference: the CPU restatement timed per step on a bounded sample."""
     from sbpom_letkf_v2_b200.synthetic import WORKLOADS, make_case
     if rank != 0:
         return
     dev = "cuda:0" if torch.cuda.is_available() else "cpu"
-    wl = WORKLOADS[args.workload]
+    wl = scaled_workload(WORKLOADS[args.workload], args.scale)
     case = make_case(wl, device=dev, seed=wl.seed)
     p = case.params.replace(precision=0)
     vals = []
@@ -198,6 +208,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=8.0)
+    ap.add_argument("--scale", type=int, default=1,
+                    help="divide nlon and nlat by S and the obs counts by S^2 (same obs density; "
+                         "for profiling runs)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -225,7 +238,7 @@ def main():
 
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
-    wl = WORKLOADS[args.workload]
+    wl = scaled_workload(WORKLOADS[args.workload], args.scale)
     case = make_case(wl, device=dev, seed=wl.seed + rank)
     prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
     p = case.params.replace(precision=prec)

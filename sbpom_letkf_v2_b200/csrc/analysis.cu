@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nvt = p.nv3d + (surf ? p.nv2d : 0);
   const bool dual = !primal && nacc > 0;
   const int n = nacc;
-  const int ldz = KP + 1, ldn = n | 1;
+  const int ldz = KP + 1, ldn = eig_ld(n);
   double *Z = S.u, *Nb = S.u + (long)ndm * ldz;
   const double alpha_d = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
   if (dual) {
@@ -224,25 +224,19 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncthreads();
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
-    bits |= jacobi_eig(Nb, n, ldn, tol, p.max_sweeps, S.lam, S.iws + 40);
-    if (tid < n) {  // c = Lambda^-1 Q^T d
-      const double *qj = Nb + (long)tid * ldn;
-      double s = 0.0;
-      for (int o = 0; o < n; ++o) s = fma(qj[o], S.b[o], s);
-      S.c[tid] = s / S.lam[tid];
-    }
+    bits |= jacobi_eig<(KP / 4 < 16 ? KP / 4 : 16)>(Nb, n, ldn, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+    vt_times(Nb, n, ldn, S.b, S.c);  // c = Lambda^-1 Q^T d
+    __syncthreads();
+    if (tid < n) S.c[tid] /= S.lam[tid];
   }
   if (!dual && nacc > 0 && do_gram) {
     const double alpha = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
     store_gram<R>(S, k, alpha, A);
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
-    bits |= jacobi_eig(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40);
-    if (tid < k) {  // c = Lambda^-1 V^T b
-      const double *vj = S.u + (long)tid * S.ldb;
-      double s = 0.0;
-      for (int m = 0; m < k; ++m) s = fma(vj[m], S.b[m], s);
-      S.c[tid] = s / S.lam[tid];
-    }
+    bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+    vt_times(S.u, k, S.ldb, S.b, S.c);  // c = Lambda^-1 V^T b
+    __syncthreads();
+    if (tid < k) S.c[tid] /= S.lam[tid];
   }
   if (do_pf && tid < k) S.ll[tid] = A.ll;
 
@@ -315,15 +309,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncthreads();
   } else if (nacc > 0 && do_gram) {
-    // T = dX V
-    for (int e = tid; e < nvt * k; e += kThreads) {
-      const int v = e / k, j = e - v * k;
-      const double *vj = B + (long)j * S.ldb;
-      const double *xv = S.x + v * KP;
-      double s = 0.0;
-      for (int m = 0; m < k; ++m) s = fma(xv[m], vj[m], s);
-      S.t[v * KP + j] = s;
-    }
+    x_times_v(S.x, KP, nvt, B, k, S.ldb, S.t, KP);  // T = dX V
     __syncthreads();
     {  // mean increment dX wvec = T c (LETKF), or dX w_gm (LPFGM)
       const int lane = tid & 31, wid = tid >> 5;

@@ -64,13 +64,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       const double alpha = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
       store_gram<R>(S, k, alpha, A);
       const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
-      bits |= jacobi_eig(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40);
-      if (tid < k) {
-        const double *vj = S.u + (long)tid * S.ldb;
-        double s = 0.0;
-        for (int m = 0; m < k; ++m) s = fma(vj[m], S.b[m], s);
-        S.c[tid] = s / S.lam[tid];
-      }
+      bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+      vt_times(S.u, k, S.ldb, S.b, S.c);
+      __syncthreads();
+      if (tid < k) S.c[tid] /= S.lam[tid];
       __syncthreads();
       const double *B = S.u;
       if (tid < k) {  // w = V c  (wvec for LETKF, w_gm for LPFGM)

@@ -23,6 +23,8 @@ __host__ __device__ constexpr int kp_of_r(int r) { return 16 * r; }
 inline int r_for_k(int k) { return k <= 32 ? 2 : k <= 64 ? 4 : k <= 112 ? 7 : 8; }
 
 constexpr int kDrawBatch = 64;  // PF draws resolved per pass
+// Leading dimension of an n x n eigensolver matrix: 4 (mod 16) doubles.
+__host__ __device__ inline int eig_ld(int n) { return (n + 15) / 16 * 16 + 4; }
 
 // Shared-memory carve of one per-point CTA (all sizes in bytes, 16-aligned).
 struct PointSmem {
@@ -41,8 +43,9 @@ struct PointSmem {
   __host__ __device__ static size_t union_bytes(int k, int kp) {
     const size_t nd = (size_t)dual_max(k);
     size_t chunk = sizeof(double) * kChunk * kp;
-    size_t mat = sizeof(double) * (size_t)k * (kp + 1);
-    size_t dual = sizeof(double) * (nd * (kp + 1) + nd * (nd + 1));
+    const size_t kk = (size_t)k;
+    size_t mat = sizeof(double) * kk * eig_ld(kp);
+    size_t dual = sizeof(double) * (nd * (kp + 1) + nd * eig_ld((int)nd));
     size_t pf = (size_t)kDrawBatch * k * (sizeof(int16_t) + 1) + 16;
     size_t m = chunk > mat ? chunk : mat;
     m = m > dual ? m : dual;
@@ -82,7 +85,7 @@ struct PointSmem {
     an = (double *)take(sizeof(double) * kNvMax * kp);
     w = (double *)take(sizeof(double) * kNvMax * kp);
     u = (double *)q;
-    ldb = kp + 1;  // odd stride: row and column walks are bank-conflict free
+    ldb = eig_ld(kp);  // 4 (mod 16): bank-conflict-free Jacobi column groups
   }
 };
 
@@ -158,22 +161,131 @@ __device__ __forceinline__ void store_gram(const PointSmem &S, int k, double alp
   __syncthreads();
 }
 
-// One-sided cyclic Jacobi on the SPD matrix in B (n x n, column-major,
-// stride ldb, n <= 128).  Round-robin ordering: in each of the n2-1 rounds the
-// n2/2 column pairs are disjoint and are processed concurrently, one 8-lane
-// group per pair (4 pairs per warp).  A pair (p,q) is rotated when
-// |b_p.b_q| > tol |b_p||b_q|; the sweep loop ends after a sweep without
-// rotations.  On return B holds the eigenvectors as columns and lam[] the
-// eigenvalues (column norms).  Returns status bits (uniform over the CTA).
-static __device__ __noinline__ int jacobi_eig(double *B, int n, int ldb, double tol, int maxsw, double *lam,
-                                              int *flag) {
-  constexpr int G = 8, E = 16;  // lanes per pair, elements per lane (n <= G*E)
+// ---------------------------------------------------------------------------
+// Symmetric eigensolver of the SPD matrix A (n x n, column-major, stride ldb)
+// held in shared memory.  Replaces mtx_eigen / DSYEV (common.f90:992-1050);
+// A >= alpha I > 0, so the reference's negative-eigenvalue branch never fires.
+//
+//  1. Cholesky with diagonal pivoting, P A P^T = L L^T, in place.
+//  2. One-sided cyclic Jacobi on the columns of L: L W -> columns that are
+//     mutually orthogonal.  Since L = V' S U^T (SVD), the converged columns are
+//     s_j v'_j: normalised, they are the eigenvectors of P A P^T, and
+//     lambda_j = s_j^2 = |column j|^2.  Un-permuting the rows gives A's.
+//     This is the preconditioned one-sided Jacobi SVD (Drmac & Veselic 2008):
+//     the sweep count follows A's spectrum (one-sided Jacobi on A itself acts
+//     on A^2, whose squared gaps near the alpha cluster need many more
+//     sweeps), and the pivoted factor's columns start nearly orthogonal.
+//
+// Jacobi detail: round-robin ordering; in each of the n2-1 rounds the n2/2
+// disjoint column pairs are processed at once, one 4-lane group per pair, 8
+// pairs per warp.  The stride ldb = 4 (mod 16) doubles puts the 8 groups'
+// 4-double segments of consecutive columns on disjoint banks.  Column norms
+// are carried in nrm[] (recomputed each sweep), so only b_p.b_q is a dot
+// product.  A pair is rotated when (b_p.b_q)^2 > tol^2 |b_p|^2 |b_q|^2; the
+// angle t is computed in FP32 while c = 1/sqrt(1+t^2), s = c t are FP64, so
+// every rotation is orthogonal to FP64 rounding and the angle only has to
+// shrink b_p.b_q (the residual of a rotation is ~1e-7 of what it removes).
+// A sweep whose largest relative b_p.b_q was below 1e-10 leaves the columns
+// orthogonal to working precision, so the loop ends after it.
+// ---------------------------------------------------------------------------
+
+// In-place pivoted Cholesky of the full symmetric matrix in B: on return B's
+// lower triangle holds L (P A P^T = L L^T), the strict upper triangle is zero
+// and perm[i] is the original index of row i.  vec: n doubles of scratch.
+static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *perm, double *vec, int *flag) {
+  const int tid = threadIdx.x, nt = blockDim.x, tx = tid & 15, ty = tid >> 4, nty = nt >> 4;
+  const int lane = tid & 31, wid = tid >> 5;
+  for (int i = tid; i < n; i += nt) perm[i] = i;
+  if (tid == 0) flag[1] = 0;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (wid == 0) {  // pivot: largest remaining diagonal (first on ties)
+      double best = -1.0;
+      int bi = j;
+      for (int i = j + lane; i < n; i += 32) {
+        const double d = B[(long)i * ldb + i];
+        if (d > best) {
+          best = d;
+          bi = i;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (lane == 0) flag[2] = bi;
+    }
+    __syncthreads();
+    const int pv = flag[2];
+    if (pv != j) {  // symmetric swap of rows / columns j and pv
+      for (int c = tid; c < n; c += nt) {
+        double *bc = B + (long)c * ldb;
+        const double t = bc[j];
+        bc[j] = bc[pv];
+        bc[pv] = t;
+      }
+      __syncthreads();
+      for (int r = tid; r < n; r += nt) {
+        const double t = B[(long)j * ldb + r];
+        B[(long)j * ldb + r] = B[(long)pv * ldb + r];
+        B[(long)pv * ldb + r] = t;
+      }
+      if (tid == 0) {
+        const int t = perm[j];
+        perm[j] = perm[pv];
+        perm[pv] = t;
+      }
+      __syncthreads();
+    }
+    double d = B[(long)j * ldb + j];
+    const bool bad = !(d > 0.0) || !isfinite(d);
+    if (bad) d = 1.0;
+    const double r = sqrt(d), inv = 1.0 / r;
+    double *bj = B + (long)j * ldb;
+    for (int i = j + 1 + tid; i < n; i += nt) vec[i] = bj[i] * inv;
+    __syncthreads();
+    if (tid == 0) {
+      bj[j] = r;
+      if (bad) flag[1] |= SBLETKF_ERR_NONFINITE;
+    }
+    for (int i = j + 1 + tid; i < n; i += nt) bj[i] = vec[i];
+    for (int c = j + 1 + ty; c < n; c += nty) {  // full symmetric trailing update
+      const double vc = vec[c];
+      double *bc = B + (long)c * ldb;
+      for (int i = j + 1 + tx; i < n; i += 16) bc[i] = fma(-vec[i], vc, bc[i]);
+    }
+    __syncthreads();
+  }
+  for (int c = ty; c < n; c += nty)
+    for (int i = tx; i < c; i += 16) B[(long)c * ldb + i] = 0.0;
+  __syncthreads();
+  return flag[1];
+}
+
+// Jacobi sweeps on the columns of B (shared memory); E = elements per lane
+// (n <= 4E).  nrm: n doubles of scratch.  flag: >= 3 shared ints.
+template <int E>
+static __device__ __forceinline__ int jacobi_sweeps(double *B, int n, int ldb, double tol, int maxsw, double *nrm,
+                                                    int *flag) {
+  constexpr int G = 4;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int grp = lane / G, gl = lane % G, lead = grp * G;
   const int n2 = (n + 1) & ~1, m = n2 - 1, npair = n2 / 2;
-  int bits = 0, sweep = 0;
-  if (threadIdx.x == 0) flag[1] = 0;
+  const double tol2 = tol * tol, big2 = 1e-20;
+  int sweep = 0;
   for (; sweep < maxsw; ++sweep) {
+    for (int j = wid; j < n; j += nw) {  // exact column norms at the start of a sweep
+      const double *cj = B + (long)j * ldb;
+      double s = 0.0;
+      for (int r = lane; r < n; r += 32) s = fma(cj[r], cj[r], s);
+      s = __shfl_sync(0xffffffffu, warp_sum(s), 0);
+      if (lane == 0) nrm[j] = s;
+    }
     if (threadIdx.x == 0) *flag = 0;
     __syncthreads();
     for (int rd = 0; rd < m; ++rd) {
@@ -184,36 +296,35 @@ static __device__ __noinline__ int jacobi_eig(double *B, int n, int ldb, double 
           a = m;
           b = rd;
         } else {
-          a = (rd + pi) % m;
-          b = (rd - pi + m) % m;
+          a = rd + pi;
+          if (a >= m) a -= m;
+          b = rd - pi;
+          if (b < 0) b += m;
         }
         const bool act = pi < npair && a < n && b < n;
         double *ca = B + (long)(act ? a : 0) * ldb, *cb = B + (long)(act ? b : 0) * ldb;
-        double va[E], vb[E], al = 0.0, be = 0.0, ga = 0.0;
+        double va[E], vb[E], g0 = 0.0, g1 = 0.0;
 #pragma unroll
         for (int t = 0; t < E; ++t) {
           const int r = gl + G * t;
           const bool in = act && r < n;
           va[t] = in ? ca[r] : 0.0;
           vb[t] = in ? cb[r] : 0.0;
-          al = fma(va[t], va[t], al);
-          be = fma(vb[t], vb[t], be);
-          ga = fma(va[t], vb[t], ga);
+          if (t & 1) g1 = fma(va[t], vb[t], g1);
+          else g0 = fma(va[t], vb[t], g0);
         }
+        double ga = g0 + g1;
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) {
-          al += __shfl_xor_sync(0xffffffffu, al, o);
-          be += __shfl_xor_sync(0xffffffffu, be, o);
-          ga += __shfl_xor_sync(0xffffffffu, ga, o);
-        }
+        for (int o = G / 2; o > 0; o >>= 1) ga += __shfl_xor_sync(0xffffffffu, ga, o);
         // one value per group, so every lane of a pair applies the same rotation
-        al = __shfl_sync(0xffffffffu, al, lead);
-        be = __shfl_sync(0xffffffffu, be, lead);
         ga = __shfl_sync(0xffffffffu, ga, lead);
-        if (act && fabs(ga) > tol * sqrt(al * be)) {
-          const double zeta = (be - al) / (2.0 * ga);
-          const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          const double cs = 1.0 / sqrt(1.0 + tt * tt), sn = cs * tt;
+        const double al = act ? nrm[a] : 1.0, be = act ? nrm[b] : 1.0;
+        const double g2 = ga * ga, ab = al * be;
+        if (act && g2 > tol2 * ab) {
+          const float zf = __fdividef((float)(be - al) * 0.5f, (float)ga);
+          const float tf = copysignf(1.0f, zf) / (fabsf(zf) + sqrtf(fmaf(zf, zf, 1.0f)));
+          const double tt = (double)tf;
+          const double cs = rsqrt(fma(tt, tt, 1.0)), sn = cs * tt;
 #pragma unroll
           for (int t = 0; t < E; ++t) {
             const int r = gl + G * t;
@@ -222,7 +333,12 @@ static __device__ __noinline__ int jacobi_eig(double *B, int n, int ldb, double 
               cb[r] = sn * va[t] + cs * vb[t];
             }
           }
-          if (gl == 0) *flag = 1;
+          if (gl == 0) {
+            const double c2 = cs * cs, s2 = sn * sn, csg = 2.0 * cs * sn * ga;
+            nrm[a] = c2 * al - csg + s2 * be;
+            nrm[b] = s2 * al + csg + c2 * be;
+            if (g2 > big2 * ab) *flag = 1;
+          }
         }
       }
       __syncthreads();
@@ -231,23 +347,88 @@ static __device__ __noinline__ int jacobi_eig(double *B, int n, int ldb, double 
     __syncthreads();
     if (!rot) break;
   }
-  if (sweep >= maxsw) bits |= SBLETKF_ERR_EIG_NOCONV;
+  __syncthreads();
+  return sweep >= maxsw ? SBLETKF_ERR_EIG_NOCONV : 0;
+}
+
+// Eigenpairs of the SPD matrix in B: eigenvectors replace B's columns and
+// lam[] receives the eigenvalues.  vec: n doubles, perm: n ints of scratch;
+// flag: >= 3 shared ints.  Returns status bits.
+template <int EMAX>
+static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, double tol, int maxsw, double *lam,
+                                                 int *flag, int *perm, double *vec) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int bits = chol_pivot(B, n, ldb, perm, vec, flag);
+  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps<8>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, maxsw, vec, flag);
+  else bits |= jacobi_sweeps<EMAX>(B, n, ldb, tol, maxsw, vec, flag);
+  // lambda_j = |column j|^2; eigenvector = column / |column|, rows un-permuted
   for (int j = wid; j < n; j += nw) {
     double *cj = B + (long)j * ldb;
-    double s = 0.0;
-    for (int r = lane; r < n; r += 32) s = fma(cj[r], cj[r], s);
+    double v[4], s = 0.0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int r = lane + 32 * t;
+      v[t] = r < n ? cj[r] : 0.0;
+      s = fma(v[t], v[t], s);
+    }
     s = __shfl_sync(0xffffffffu, warp_sum(s), 0);
-    const double l = sqrt(s);
-    if (lane == 0) lam[j] = l;
-    const double inv = 1.0 / l;
-    for (int r = lane; r < n; r += 32) cj[r] *= inv;
+    if (lane == 0) lam[j] = s;
+    const double inv = 1.0 / sqrt(s);
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int r = lane + 32 * t;
+      if (r < n) cj[perm[r]] = v[t] * inv;
+    }
   }
+  if (threadIdx.x == 0) flag[1] = 0;
   __syncthreads();
   for (int j = threadIdx.x; j < n; j += blockDim.x)
     if (!(lam[j] > 0.0) || !isfinite(lam[j])) atomicOr(flag + 1, SBLETKF_ERR_NONFINITE);
   __syncthreads();
   bits |= flag[1];
   return bits;
+}
+
+// out[v*ldo + j] = sum_m X[v*ldx + m] V[m][j] for v < nv, j < n: warp per
+// column j, lanes over rows m (contiguous in a column of V).
+static __device__ __forceinline__ void x_times_v(const double *X, int ldx, int nv, const double *V, int n, int ldb,
+                                                 double *out, int ldo) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = wid; j < n; j += nw) {
+    const double *vj = V + (long)j * ldb;
+    double acc[kNvMax];
+#pragma unroll
+    for (int v = 0; v < kNvMax; ++v) acc[v] = 0.0;
+    for (int r = lane; r < n; r += 32) {
+      const double vr = vj[r];
+#pragma unroll
+      for (int v = 0; v < kNvMax; ++v)
+        if (v < nv) acc[v] = fma(X[v * ldx + r], vr, acc[v]);
+    }
+#pragma unroll
+    for (int v = 0; v < kNvMax; ++v) {
+      if (v < nv) {
+        const double t = __shfl_sync(0xffffffffu, warp_sum(acc[v]), 0);
+        if (lane == 0) out[v * ldo + j] = t;
+      }
+    }
+  }
+}
+
+// out[j] = sum_m V[m][j] x[m] (j < n), warp per column, lanes over rows.
+static __device__ __forceinline__ void vt_times(const double *V, int n, int ldb, const double *x, double *out) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = wid; j < n; j += nw) {
+    const double *vj = V + (long)j * ldb;
+    double s = 0.0;
+    for (int r = lane; r < n; r += 32) s = fma(vj[r], x[r], s);
+    s = __shfl_sync(0xffffffffu, warp_sum(s), 0);
+    if (lane == 0) out[j] = s;
+  }
 }
 
 // Normalised weights and their serial cumulative sum into S.cw
