@@ -48,6 +48,7 @@ extern "C" {
 #define SBLETKF_ERR_EIG_NEG     64  /* all eigenvalues negative (common.f90:1031) */
 #define SBLETKF_ERR_ROWS        128 /* local search box has too many grid rows  */
 #define SBLETKF_ERR_UNSUPPORTED 256 /* option not supported by this entry point */
+#define SBLETKF_ERR_TIMEOUT     512 /* a bounded device wait expired            */
 
 /* ---- enumerations ----------------------------------------------------- */
 #define SBLETKF_F32 0               /* dtype codes */

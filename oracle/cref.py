@@ -7,9 +7,14 @@ dgemm / sgemm / dsyev through scipy's cython_blas / cython_lapack capsules.
 """
 from __future__ import annotations
 
-import ctypes
 import os
-import subprocess
+
+# The restatement calls BLAS from its own OpenMP threads; OpenBLAS must not
+# start threads of its own (it reads this when scipy first loads it).
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
+import ctypes  # noqa: E402
+import subprocess  # noqa: E402
 
 import numpy as np
 

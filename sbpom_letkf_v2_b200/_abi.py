@@ -17,10 +17,12 @@ LIB_PATH = os.path.join(HERE, "libsbletkf.so")
 OK = 0
 ERR_ARG, ERR_CUDA, ERR_WORKSPACE, ERR_OBS_CELL = 1, 2, 4, 8
 ERR_EIG_NOCONV, ERR_NONFINITE, ERR_EIG_NEG, ERR_ROWS, ERR_UNSUPPORTED = 16, 32, 64, 128, 256
+ERR_TIMEOUT = 512
 _NAMES = {ERR_ARG: "bad argument", ERR_CUDA: "CUDA error", ERR_WORKSPACE: "workspace too small",
           ERR_OBS_CELL: "obs cell index out of range", ERR_EIG_NOCONV: "Jacobi sweep cap reached",
           ERR_NONFINITE: "non-finite value", ERR_EIG_NEG: "all eigenvalues negative",
-          ERR_ROWS: "search box has too many rows", ERR_UNSUPPORTED: "unsupported option"}
+          ERR_ROWS: "search box has too many rows", ERR_UNSUPPORTED: "unsupported option",
+          ERR_TIMEOUT: "bounded device wait expired"}
 
 #: every symbol include/sbletkf.h declares
 EXPORTS = ("sbletkf_abi_version", "sbletkf_workspace_create", "sbletkf_workspace_destroy",

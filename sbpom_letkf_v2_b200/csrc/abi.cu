@@ -137,7 +137,6 @@ int sbletkf_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const sblet
   if (p->nv3d > 0 && (!fcst3d || !anal3d)) return SBLETKF_ERR_ARG;
   if (p->nv2d > 0 && (!fcst2d || !anal2d)) return SBLETKF_ERR_ARG;
   if (p->iswitch_da != SBLETKF_DA_LETKF && !uniforms && ws->nobs > 0) return SBLETKF_ERR_ARG;
-  if (p->precision == SBLETKF_PREC_MIXED) return SBLETKF_ERR_UNSUPPORTED;
   if (cudaSetDevice(ws->device) != cudaSuccess) return SBLETKF_ERR_CUDA;
   cudaStream_t s = (cudaStream_t)stream;
   if (ws->nobs == 0) {  // common_da.f90:57-61: analysis = forecast, no round-off

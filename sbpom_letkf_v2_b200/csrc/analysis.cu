@@ -23,7 +23,133 @@
 namespace sbl {
 namespace {
 
-template <int R, typename ST>
+// State of the tensor-core Gram pipeline of one CTA (uniform across threads).
+struct TcState {
+  uint32_t tbase;   // TMEM base: C1 at column 0, C2 at column KP
+  int uses[2];      // commits issued per operand stage
+  int nchunk;
+  int broken;       // a wait timed out: issue nothing more
+};
+
+// Stage `cnt` list entries starting at f as BF16 hi/lo operand tiles and issue
+// their two UMMAs per K-block (C1 += Zh^T Zh, C2 += Zh^T Zl).  Also
+// accumulates b = sum w dep y (FP64) and, when do_pf, the PF log-likelihood.
+// Whole CTA; ends with the tiles handed to the tensor core.
+template <int KP>
+__device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, TcState &st, uint64_t *mbar,
+                                         int f, int cnt, int k, bool do_pf, double &bacc, double &llacc,
+                                         int &bits) {
+  using namespace tc;
+  const int tid = threadIdx.x;
+  const int s = st.nchunk & 1;
+  float *stg = reinterpret_cast<float *>(S.u);  // [kKC][KP] FP32 rows
+  unsigned char *tiles = reinterpret_cast<unsigned char *>(S.u) + PointSmem::tc_tiles_off(KP);
+  unsigned char *hi = tiles + s * kStageBytes, *lo = hi + kTileBytes;
+  float *sw = reinterpret_cast<float *>(S.cw);
+  __shared__ int s_broken;
+  if (tid == 0) {  // the stage's previous UMMAs must be done
+    if (!st.broken && st.uses[s] > 0 && !mbar_wait(&mbar[s], (uint32_t)((st.uses[s] - 1) & 1))) {
+      bits |= SBLETKF_ERR_TIMEOUT;
+      s_broken = 1;
+    } else {
+      s_broken = st.broken;
+    }
+  }
+  constexpr int KP4 = KP / 4;
+  for (int e = tid; e < kKC * KP4; e += kThreads) {
+    const int cc = e / KP4, col = e - cc * KP4;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (cc < cnt) v = reinterpret_cast<const float4 *>(ob.hdxf32 + (long)S.lidx[f + cc] * ob.ldh)[col];
+    reinterpret_cast<float4 *>(stg)[e] = v;
+  }
+  if (tid < kKC) sw[tid] = tid < cnt ? (float)sqrt(S.lw[f + tid]) : 0.0f;
+  __syncthreads();
+  st.broken = s_broken;
+  if (tid < KP)
+    for (int cc = 0; cc < cnt; ++cc) bacc = fma(S.lwd[f + cc], (double)stg[cc * KP + tid], bacc);
+  if (do_pf && tid < k) {
+    for (int cc = 0; cc < cnt; ++cc) {
+      double d = __dsub_rn(S.ldep[f + cc], (double)stg[cc * KP + tid]);
+      double q = __dmul_rn(__dmul_rn(0.5, d), d);
+      q = __ddiv_rn(__dmul_rn(q, S.lrloc[f + cc]), S.lrdiag[f + cc]);
+      llacc = __dsub_rn(llacc, q);
+    }
+  }
+  for (int e = tid; e < kM * (kKC / 8); e += kThreads) {
+    const int m = e & (kM - 1), g = e >> 7;
+    float z[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int o = g * 8 + i;
+      z[i] = m < KP ? sw[o] * stg[o * KP + m] : 0.0f;
+    }
+    store_split8(hi, lo, tile_off(m, g * 8), z);
+  }
+  fence_async_smem();
+  __syncthreads();
+  if (tid == 0 && !st.broken) {
+    fence_after_sync();
+    const uint32_t idesc = idesc_bf16(kM, KP);
+    const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
+#pragma unroll
+    for (int kb = 0; kb < kKC / kKB; ++kb) {
+      const uint64_t da = sdesc(ah + kb * kBlockBytes), dl = sdesc(al + kb * kBlockBytes);
+      const uint32_t acc = (st.nchunk > 0 || kb > 0) ? 1u : 0u;
+      mma_bf16(st.tbase, da, da, idesc, acc);
+      mma_bf16(st.tbase + KP, da, dl, idesc, acc);
+    }
+    commit_to(&mbar[s]);
+  }
+  st.uses[s]++;
+  st.nchunk++;
+}
+
+// Wait for every issued UMMA, then G = C1 + C2 + C2^T + alpha I into B (FP64,
+// column-major, stride ldb) and b into S.b.
+template <int KP>
+__device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint64_t *mbar, int k, double alpha,
+                                          double bacc, int &bits) {
+  using namespace tc;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) {
+    for (int s = 0; s < 2; ++s)
+      if (!st.broken && st.uses[s] > 0 && !mbar_wait(&mbar[s], (uint32_t)((st.uses[s] - 1) & 1))) {
+        bits |= SBLETKF_ERR_TIMEOUT;
+        st.broken = 1;
+      }
+  }
+  __syncthreads();
+  fence_after_sync();
+  double *B = S.u;
+  const int q = wid & 3, half = wid >> 2, r = 32 * q + lane;
+  const uint32_t trow = st.tbase + ((uint32_t)(32 * q) << 16);
+  float v1[16], v2[16];
+  for (int ch = half; ch < KP / 16; ch += 2) {  // pass 1: row r of C1 + C2
+    tmem_ld16(trow + 16 * ch, v1);
+    tmem_ld16(trow + KP + 16 * ch, v2);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int c = 16 * ch + i;
+      if (r < k && c < k) B[(long)c * S.ldb + r] = (double)v1[i] + (double)v2[i] + (r == c ? alpha : 0.0);
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  for (int ch = half; ch < KP / 16; ch += 2) {  // pass 2: + C2^T, thread r owns column r
+    tmem_ld16(trow + KP + 16 * ch, v2);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const int c = 16 * ch + i;
+      if (r < k && c < k) B[(long)r * S.ldb + c] += (double)v2[i];
+    }
+  }
+  if (tid < k) S.b[tid] = bacc;
+  fence_before_sync();
+  __syncthreads();
+}
+
+template <int R, typename ST, bool MIXED>
 __global__ void __launch_bounds__(kThreads, 1)
     k_analysis(const sbletkf_params p, const GridView g, const ObsView ob, const ST *__restrict__ f3,
                const ST *__restrict__ f2, ST *__restrict__ a3, ST *__restrict__ a2, const double *__restrict__ uni,
@@ -41,7 +167,33 @@ __global__ void __launch_bounds__(kThreads, 1)
   const bool do_gram = p.iswitch_da != SBLETKF_DA_LPF;
   __shared__ int sh[8];
   __shared__ double shd[4];
+  __shared__ uint64_t s_mbar[2];
+  __shared__ uint32_t s_tmem;
   int bits = 0;
+  constexpr uint32_t kTmemCols = (2 * KP <= 64) ? 64 : (2 * KP <= 128) ? 128 : 256;
+  const bool use_tc = MIXED && do_gram;
+  TcState tcs;
+  tcs.uses[0] = tcs.uses[1] = 0;
+  tcs.nchunk = 0;
+  tcs.tbase = 0;
+  tcs.broken = 0;
+  if (use_tc) {
+    // after a tensor-core wait has timed out anywhere in the launch, later
+    // CTAs return at once (the status word already carries the error)
+    __shared__ int s_abort;
+    if (tid == 0) s_abort = (*(volatile int *)status & SBLETKF_ERR_TIMEOUT) != 0;
+    __syncthreads();
+    if (s_abort) {
+      if (tid == 0 && pst) pst[pid] = SBLETKF_ERR_TIMEOUT;
+      return;
+    }
+    if ((tid >> 5) == 0) tc::tmem_alloc(&s_tmem, kTmemCols);
+    if (tid == 0) {
+      tc::mbar_init(&s_mbar[0], 1);
+      tc::mbar_init(&s_mbar[1], 1);
+    }
+    tc::fence_before_sync();
+  }
 
   // ---- search box and its grid rows (common_da.f90:158-161, 314-346)
   if (tid == 0) {
@@ -63,6 +215,10 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   __syncthreads();
   bits |= sh[5];
+  if (use_tc) {
+    tc::fence_after_sync();
+    tcs.tbase = s_tmem;
+  }
   const int imin = sh[0], imax = sh[1], jmin = sh[2], nrows = sh[4];
   const double rdep = shd[0], plon = shd[1], plat = shd[2], phi = shd[3];
   {
@@ -143,7 +299,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (!primal && L > ndm) primal = true;
     if (!primal) continue;
     int f = 0;
-    while (L - f >= kChunk) {
+    if (use_tc) {
+      while (L - f >= tc::kKC) {
+        tc_chunk<KP>(S, ob, tcs, s_mbar, f, tc::kKC, k, do_pf, A.b, A.ll, bits);
+        f += tc::kKC;
+      }
+    }
+    while (!use_tc && L - f >= kChunk) {
       constexpr int KP2 = KP / 2;
       for (int e = tid; e < kChunk * KP2; e += kThreads) {
         const int cc = e / KP2, col = e - cc * KP2;
@@ -169,7 +331,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     L = rem;
   }
-  if (primal && L > 0) {
+  if (use_tc && primal && L > 0) tc_chunk<KP>(S, ob, tcs, s_mbar, 0, L, k, do_pf, A.b, A.ll, bits);
+  if (!use_tc && primal && L > 0) {
     constexpr int KP2 = KP / 2;
     for (int e = tid; e < L * KP2; e += kThreads) {
       const int cc = e / KP2, col = e - cc * KP2;
@@ -231,7 +394,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   if (!dual && nacc > 0 && do_gram) {
     const double alpha = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
-    store_gram<R>(S, k, alpha, A);
+    if (use_tc) tc_finish<KP>(S, tcs, s_mbar, k, alpha, A.b, bits);
+    else store_gram<R>(S, k, alpha, A);
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
     bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
     vt_times(S.u, k, S.ldb, S.b, S.c);  // c = Lambda^-1 V^T b
@@ -396,6 +560,21 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (v < p.nv3d) a3[(((long)v * k + m) * nlev + kl) * nij1 + i] = (ST)a;
     else a2[((long)(v - p.nv3d) * k + m) * nij1 + i] = (ST)a;
   }
+  if (use_tc && (bits & SBLETKF_ERR_TIMEOUT)) atomicOr(status, SBLETKF_ERR_TIMEOUT);
+  if (use_tc) {  // every UMMA was waited for in tc_finish (or never issued)
+    tc::fence_before_sync();
+    __syncthreads();
+    if ((tid >> 5) == 0) {
+      tc::fence_after_sync();
+      tc::tmem_dealloc(tcs.tbase, kTmemCols);
+    }
+  }
+  __shared__ int s_bits;
+  if (tid == 0) s_bits = 0;
+  __syncthreads();
+  if (bits) atomicOr(&s_bits, bits);
+  __syncthreads();
+  bits = s_bits;
   if (tid == 0) {
     if (pst) pst[pid] = bits;
     if (bits) atomicOr(status, bits);
@@ -430,11 +609,11 @@ __global__ void k_count(const sbletkf_params p, const GridView g, const ObsView 
   (void)status;
 }
 
-template <int R, typename ST>
+template <int R, typename ST, bool MIXED>
 int launch_r(const sbletkf_params *p, const GridView &g, const ObsView &ob, const void *f3, const void *f2, void *a3,
              void *a2, const double *uni, int32_t *src, int32_t *pst, int *status, cudaStream_t s) {
-  const size_t smem = PointSmem::bytes(p->nmem, kp_of_r(R));
-  auto kern = k_analysis<R, ST>;
+  const size_t smem = PointSmem::bytes(p->nmem, kp_of_r(R), MIXED);
+  auto kern = k_analysis<R, ST, MIXED>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_status(e);
   const long long P = (long long)p->nlev * g.nij1;
@@ -450,11 +629,16 @@ int launch_r(const sbletkf_params *p, const GridView &g, const ObsView &ob, cons
 template <typename ST>
 int launch_t(const sbletkf_params *p, const GridView &g, const ObsView &ob, const void *f3, const void *f2, void *a3,
              void *a2, const double *uni, int32_t *src, int32_t *pst, int *status, cudaStream_t s) {
+  const bool mixed = p->precision == SBLETKF_PREC_MIXED;
   switch (r_for_k(p->nmem)) {
-    case 2: return launch_r<2, ST>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
-    case 4: return launch_r<4, ST>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
-    case 7: return launch_r<7, ST>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
-    default: return launch_r<8, ST>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+    case 2: return mixed ? launch_r<2, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s)
+                         : launch_r<2, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+    case 4: return mixed ? launch_r<4, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s)
+                         : launch_r<4, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+    case 7: return mixed ? launch_r<7, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s)
+                         : launch_r<7, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+    default: return mixed ? launch_r<8, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s)
+                          : launch_r<8, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
   }
 }
 

@@ -1,0 +1,137 @@
+// gram_tc.cuh -- the local Gram Y^T diag(rloc/rdiag) Y on the 5th-generation
+// tensor cores (tcgen05, sm_100a), split-precision BF16.
+//
+// With z_o = sqrt(rloc_o/rdiag_o) y_o the Gram is G = Z^T Z.  Each row is split
+// into z = hi + lo with hi = bf16(z), lo = bf16(z - hi) (16 significant bits),
+// and G ~= Zh^T Zh + Zh^T Zl + Zl^T Zh = C1 + C2 + C2^T: two UMMAs per K-block
+// accumulate C1 and C2 in FP32 in tensor memory; the dropped Zl^T Zl term is
+// below 2^-16 of G.  (common_letkf.f90:93-122 computes the same Gram with
+// sgemm/dgemm.)
+//
+// Operand tile: rows = members (M = 128, zero-padded), K = observations, in the
+// K-major canonical layout without swizzle: 8x8 "core matrices" of 8 rows x 16
+// bytes; element (row r, k) of a 16-wide K block lives at
+//   (r/8)*256 + ((k%16)/8)*128 + (r%8)*16 + (k%8)*2     (LBO = 128, SBO = 256),
+// one K block of 128 rows = 4096 bytes.  Z^T (A, M x K) and Z (B, K x N) are the
+// same tile, so one descriptor serves both operands.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "internal.cuh"
+
+namespace sbl {
+namespace tc {
+
+constexpr int kM = 128;            // UMMA M (members, zero padded)
+constexpr int kKC = 64;            // observations per staged chunk (4 K-blocks)
+constexpr int kKB = 16;            // UMMA K for kind::f16
+constexpr int kBlockBytes = kM * kKB * 2;             // one 16-wide K block, 4096 B
+constexpr int kTileBytes = kBlockBytes * (kKC / kKB);  // one chunk, hi or lo: 16 KB
+constexpr int kStageBytes = 2 * kTileBytes;            // hi + lo
+constexpr unsigned kWaitLimit = 1u << 20;              // bounded mbarrier polls
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// tcgen05 shared-memory matrix descriptor (no swizzle, K-major).
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr & 0x3FFFFu) >> 4);            // start address  [0,14)
+  d |= (uint64_t)((128u >> 4) & 0x3FFFu) << 16;       // LBO = 128 B    [16,30)
+  d |= (uint64_t)((256u >> 4) & 0x3FFFu) << 32;       // SBO = 256 B    [32,46)
+  d |= (uint64_t)1 << 46;                             // descriptor version 1 [46,48)
+  return d;                                           // base 0, layout SWIZZLE_NONE
+}
+
+// Instruction descriptor, kind::f16: D F32, A/B BF16, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols));
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dtmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void commit_to(uint64_t *mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+
+// Wait for phase `parity` of an mbarrier; false after kWaitLimit polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+  const uint32_t a = smem_u32(mbar);
+  for (unsigned it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Byte offset of (row, k) inside one chunk tile (k in [0, kKC)).
+__device__ __forceinline__ uint32_t tile_off(int row, int k) {
+  return (uint32_t)((k >> 4) * kBlockBytes + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+// Split 8 FP32 values into BF16 hi / lo and store them as two 16-byte rows of
+// the hi and lo tiles.
+__device__ __forceinline__ void store_split8(unsigned char *hi_tile, unsigned char *lo_tile, uint32_t off,
+                                             const float *z) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(z[2 * i]), h1 = __float2bfloat16_rn(z[2 * i + 1]);
+    const __nv_bfloat16 l0 = __float2bfloat16_rn(z[2 * i] - __bfloat162float(h0));
+    const __nv_bfloat16 l1 = __float2bfloat16_rn(z[2 * i + 1] - __bfloat162float(h1));
+    h[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+    l[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+  }
+  *reinterpret_cast<uint4 *>(hi_tile + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4 *>(lo_tile + off) = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+}  // namespace tc
+}  // namespace sbl

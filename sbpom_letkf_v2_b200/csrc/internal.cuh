@@ -13,7 +13,7 @@ constexpr int kRowMax = 1024;    // grid rows of one local search box
 constexpr int kThreads = 256;    // CTA size of the per-point kernels
 constexpr int kChunk = 32;       // local obs rows staged per Gram step
 constexpr int kDualMax = 64;     // local obs handled by the observation-space transform
-constexpr int kListCap = kThreads + kDualMax + kChunk;
+constexpr int kListCap = kThreads + 64 + 64;  // streaming step + max(kDualMax, chunk) + chunk
 
 // Sorted observation arrays owned by the workspace (cell order of
 // common_obs.f90:266-377).  hdxf rows are padded to ldh with zeros.

@@ -14,6 +14,7 @@
 //                      (common_lpfgm.f90:89-197)
 #pragma once
 
+#include "gram_tc.cuh"
 #include "internal.cuh"
 
 namespace sbl {
@@ -39,8 +40,15 @@ struct PointSmem {
 
   // Largest nobsl that takes the observation-space (dual) transform.
   __host__ __device__ static int dual_max(int k) { return k - 1 < kDualMax ? k - 1 : kDualMax; }
-  // Union size: max(chunk rows, k x ldb matrix, dual Z and N, draw buffers).
-  __host__ __device__ static size_t union_bytes(int k, int kp) {
+  // Offset of the tensor-core operand stages inside the union (mixed path):
+  // after the FP32 staging rows, 1024-aligned.
+  __host__ __device__ static size_t tc_tiles_off(int kp) {
+    return ((size_t)tc::kKC * kp * sizeof(float) + 1023) & ~size_t(1023);
+  }
+  // Union size: max(chunk rows, k x ldb matrix, dual Z and N, draw buffers,
+  // and for the mixed path FP32 staging + two operand stages).
+  __host__ __device__ static size_t union_bytes(int k, int kp, bool mixed = false) {
+    const size_t tcb = mixed ? tc_tiles_off(kp) + 2 * (size_t)tc::kStageBytes + 1024 : 0;
     const size_t nd = (size_t)dual_max(k);
     size_t chunk = sizeof(double) * kChunk * kp;
     const size_t kk = (size_t)k;
@@ -49,6 +57,7 @@ struct PointSmem {
     size_t pf = (size_t)kDrawBatch * k * (sizeof(int16_t) + 1) + 16;
     size_t m = chunk > mat ? chunk : mat;
     m = m > dual ? m : dual;
+    m = m > tcb ? m : tcb;
     return a16(m > pf ? m : pf);
   }
   __host__ __device__ static size_t fixed_bytes(int kp) {
@@ -60,7 +69,9 @@ struct PointSmem {
     s += 4 * a16(sizeof(double) * kNvMax * kp);
     return s;
   }
-  __host__ __device__ static size_t bytes(int k, int kp) { return fixed_bytes(kp) + union_bytes(k, kp); }
+  __host__ __device__ static size_t bytes(int k, int kp, bool mixed = false) {
+    return fixed_bytes(kp) + union_bytes(k, kp, mixed) + (mixed ? 1024 : 0);
+  }
 
   __device__ void carve(void *base, int k, int kp) {
     char *q = (char *)base;

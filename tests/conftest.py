@@ -1,6 +1,8 @@
 import os
 import sys
 
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

@@ -139,3 +139,40 @@ def test_bad_obs_cell_raises(cuda):
     ob["idx"][3] = case.params.nlon  # a cell outside [1, nlon-1]
     with pytest.raises(SBLETKFError):
         run_gpu(case.params, g, ob, f3, f2)
+
+
+# ---- mixed precision: tcgen05 BF16 hi/lo Gram, FP64 eigensolve and transform
+TOL_MIXED = 1e-4   # relative error of analysis mean and spread vs the FP64 oracle
+
+
+def _mean_spread_err(a3, ref3):
+    m, s = a3.mean(axis=1), a3.std(axis=1, ddof=1)
+    m0, s0 = ref3.mean(axis=1), ref3.std(axis=1, ddof=1)
+    em = max(np.abs(m[v] - m0[v]).max() / np.abs(m0[v]).max() for v in range(m.shape[0]))
+    es = max(np.abs(s[v] - s0[v]).max() / np.abs(s0[v]).max() for v in range(s.shape[0]))
+    return em, es
+
+
+@pytest.mark.parametrize("k", [20, 64, 100, 128])
+def test_mixed_letkf_mean_spread_within_1e4(k, cuda):
+    wl = WORKLOADS[0].scaled(nlon=24, nlat=18, nlev=6, nmem=k, n_sst=900, n_ssh=300, n_prof=8, seed=700 + k)
+    case = make_case(wl, cov_infl_mul=1.1)
+    g, ob, f3, f2 = _np(case)
+    ref = cref.da_main(case.params, g, ob, f3, f2, rsize=8)
+    r = run_gpu(case.params.replace(precision=1), g, ob, f3, f2)
+    assert (r["status"] == 0).all()
+    em, es = _mean_spread_err(r["anal3d"], ref["anal3d"])
+    assert em <= TOL_MIXED and es <= TOL_MIXED
+    em2, es2 = _mean_spread_err(r["anal2d"], ref["anal2d"])
+    assert em2 <= TOL_MIXED and es2 <= TOL_MIXED
+
+
+def test_mixed_lpfgm_within_1e4(cuda):
+    case = _case(48, iswitch_da=DA_LPFGM, rm=RM_SR, nmonte=4)
+    g, ob, f3, f2 = _np(case)
+    P = case.params.nlev * case.nij1
+    uni = pf_uniforms(P, 4, 48, RM_SR).numpy()
+    ref = cref.da_main(case.params, g, ob, f3, f2, uniforms=uni, rsize=8)
+    r = run_gpu(case.params.replace(precision=1), g, ob, f3, f2, uni=uni)
+    em, es = _mean_spread_err(r["anal3d"], ref["anal3d"])
+    assert em <= TOL_MIXED and es <= TOL_MIXED
