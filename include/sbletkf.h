@@ -201,12 +201,15 @@ int sbletkf_analysis_noalloc(const sbletkf_params *p, const sbletkf_grid *grid, 
                              int32_t state_dtype, const double *uniforms, int32_t *point_status,
                              void *stream);
 
-/* Vector-Jacobian product of the LETKF analysis (iswitch_da = 1, RTPS = 0):
- * given dJ/d anal3d and dJ/d anal2d (same layouts as the state, state_dtype),
- * accumulate dJ/d dep and dJ/d rdiag ([nobs], caller's obs order, FP64,
- * added to), dJ/d cov_infl_mul and dJ/d sigma_obs (one FP64 each, added to).
- * dist_zero is held fixed.  Recomputes each point's eigensolve.  No
- * reference counterpart (new capability). */
+/* Vector-Jacobian product of the LETKF analysis (iswitch_da = 1, with RTPP,
+ * RTPS and the T/S round-off): given dJ/d anal3d and dJ/d anal2d (same layouts
+ * as the state, state_dtype), accumulate dJ/d dep and dJ/d rdiag ([nobs],
+ * caller's obs order, FP64, added to), dJ/d cov_infl_mul and dJ/d sigma_obs
+ * (one FP64 each, added to); all four are device pointers.  dist_zero is held
+ * fixed.  Recomputes each point's eigensolve in FP64 whatever p->precision
+ * says.  nmem <= 112 (larger: SBLETKF_ERR_UNSUPPORTED).  Uses the
+ * observations of the last sbletkf_prepare_obs.  No reference counterpart
+ * (new capability). */
 int sbletkf_backward(sbletkf_workspace *ws, const sbletkf_params *p,
                      const sbletkf_grid *grid,
                      const void *fcst3d, const void *fcst2d, int32_t state_dtype,

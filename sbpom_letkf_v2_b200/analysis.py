@@ -152,6 +152,40 @@ class Analysis:
             self.raise_status(stream)
         return a3, a2
 
+    def backward(self, grid: dict, fcst3d: torch.Tensor, fcst2d: torch.Tensor, grad_anal3d: torch.Tensor,
+                 grad_anal2d: torch.Tensor, params: LETKFParams | None = None, stream=None, check: bool = True):
+        """Vector-Jacobian product of ``da_main`` (LETKF) for the observations
+        of the last ``prepare_obs``: returns FP64 (dJ/d dep [nobs], dJ/d rdiag
+        [nobs], dJ/d cov_infl_mul, dJ/d sigma_obs) in the caller's obs order,
+        with dist_zero held at its value in ``params``."""
+        if self.nobs is None:
+            raise RuntimeError("prepare_obs() must be called first")
+        p = params or self.params
+        cp = self._params(params)
+        st_dtype = fcst3d.dtype
+        if st_dtype not in (torch.float32, torch.float64):
+            raise TypeError("state must be float32 or float64")
+        f3 = _dev(fcst3d, st_dtype, self.device, "fcst3d")
+        f2 = _dev(fcst2d, st_dtype, self.device, "fcst2d")
+        g3 = _dev(grad_anal3d, st_dtype, self.device, "grad_anal3d")
+        g2 = _dev(grad_anal2d, st_dtype, self.device, "grad_anal2d")
+        if tuple(f3.shape) != (p.nv3d, p.nmem, p.nlev, self.nij1) or g3.shape != f3.shape:
+            raise ValueError("fcst3d / grad_anal3d must be [nv3d][nmem][nlev][nij1]")
+        if tuple(f2.shape) != (p.nv2d, p.nmem, self.nij1) or g2.shape != f2.shape:
+            raise ValueError("fcst2d / grad_anal2d must be [nv2d][nmem][nij1]")
+        gdep = torch.zeros(max(self.nobs, 1), dtype=torch.float64, device=self.device)
+        grd = torch.zeros_like(gdep)
+        gsc = torch.zeros(2, dtype=torch.float64, device=self.device)
+        g, cg = self._grid(grid)
+        code = self.lib.sbletkf_backward(self._ws, ctypes.byref(cp), ctypes.byref(cg), _ptr(f3), _ptr(f2),
+                                         F64 if st_dtype == torch.float64 else F32, _ptr(g3), _ptr(g2),
+                                         _ptr(gdep), _ptr(grd), _ptr(gsc), gsc.data_ptr() + 8,
+                                         _stream_ptr(stream))
+        _abi.check(code, "backward")
+        if check:
+            self.raise_status(stream)
+        return gdep[: self.nobs], grd[: self.nobs], gsc[0], gsc[1]
+
     def count_nobsl(self, grid: dict, params: LETKFParams | None = None, stream=None) -> torch.Tensor:
         """nobsl of every point as [nlev][nij1] int32 (common_da.f90:133-205)."""
         g, cg = self._grid(grid)

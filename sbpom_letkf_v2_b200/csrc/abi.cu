@@ -203,7 +203,7 @@ int sbletkf_backward(sbletkf_workspace *ws, const sbletkf_params *p, const sblet
   int st = check_params(p);
   if (st) return st;
   if (!same_shape(ws, p) || !grid_ok(grid) || grid->nij1 != ws->nij1) return SBLETKF_ERR_ARG;
-  if (p->iswitch_da != SBLETKF_DA_LETKF || p->alpha_rtps > 0.0) return SBLETKF_ERR_UNSUPPORTED;
+  if (p->iswitch_da != SBLETKF_DA_LETKF) return SBLETKF_ERR_UNSUPPORTED;
   if (!grad_dep || !grad_rdiag || !grad_infl || !grad_sigma_obs) return SBLETKF_ERR_ARG;
   if (state_dtype != SBLETKF_F32 && state_dtype != SBLETKF_F64) return SBLETKF_ERR_ARG;
   if (cudaSetDevice(ws->device) != cudaSuccess) return SBLETKF_ERR_CUDA;
