@@ -128,7 +128,36 @@ def algorithmic_flops(nobsl: np.ndarray, k: int, nv3d: int, nv2d: int, nlev: int
     return {"gram": f_gram, "eig": f_eig, "w": f_w, "upd": f_upd, "total": f_gram + f_eig + f_w + f_upd}
 
 
-def cpu_baseline(case, p, seconds: float = 15.0, nthreads: int = 0):
+def algorithmic_bytes(nobsl: np.ndarray, k: int, nv3d: int, nv2d: int, nlev: int, nij1: int) -> dict:
+    """Per-launch algorithmic HBM bytes: PF weights B_w = 4 n (k+3) per point
+    with obs (hdxf row, dep, rloc, rdiag in FP32), PF gather / ensemble update
+    B_g = B_upd = 2*4 k nv per point (read forecast, write analysis, FP32)."""
+    n = nobsl.astype(np.float64).reshape(nlev, nij1)
+    nv = np.full_like(n, nv3d, dtype=np.float64)
+    nv[nlev - 1, :] += nv2d
+    b_w = float((4.0 * n * (k + 3)).sum())
+    b_g = float((8.0 * k * nv).sum())
+    return {"weights": b_w, "gather": b_g, "total": b_w + b_g}
+
+
+def mean_spread_error(a3, a2, r3, r2) -> dict:
+    """Relative error of the analysis ensemble mean and spread of (a3, a2)
+    against (r3, r2), per variable: max |x - r| / max |r| and
+    rms(x - r) / rms(r); the worst variable is reported."""
+    out = {"mean_max": 0.0, "mean_rms": 0.0, "spread_max": 0.0, "spread_rms": 0.0}
+    for a, r in ((a3, r3), (a2, r2)):
+        for v in range(a.shape[0]):
+            x, y = a[v].double(), r[v].double()
+            for name, fx, fy in (("mean", x.mean(0), y.mean(0)), ("spread", x.std(0), y.std(0))):
+                d = fx - fy
+                mx = float(d.abs().max() / fy.abs().max().clamp_min(1e-300))
+                rms = float(torch.sqrt((d * d).mean() / (fy * fy).mean().clamp_min(1e-300)))
+                out[name + "_max"] = max(out[name + "_max"], mx)
+                out[name + "_rms"] = max(out[name + "_rms"], rms)
+    return out
+
+
+def cpu_baseline(case, p, seconds: float = 15.0, nthreads: int = 0, uniforms=None):
     """The C restatement (reference default r_size = binary32 build) on a
     stratified sample of whole grid columns, all levels; returns gridpoints/s."""
     from oracle import cref
@@ -143,8 +172,12 @@ def cpu_baseline(case, p, seconds: float = 15.0, nthreads: int = 0):
         ct = torch.as_tensor(cols, device=case.fcst3d.device)
         f3 = case.fcst3d[:, :, :, ct].cpu().numpy()
         f2 = case.fcst2d[:, :, ct].cpu().numpy()
+        uni = None
+        if uniforms is not None:  # point ids k*nij1+i -> k*ncols+j of the sampled columns
+            u = uniforms.view(p.nlev, nij1, *uniforms.shape[1:])[:, ct]
+            uni = u.reshape(p.nlev * len(cols), *uniforms.shape[1:]).cpu().numpy()
         t = time.perf_counter()
-        cref.da_main(p, g, ob, f3, f2, rsize=4, nthreads=nthreads, sorted_inputs=si)
+        cref.da_main(p, g, ob, f3, f2, uniforms=uni, rsize=4, nthreads=nthreads, sorted_inputs=si)
         return time.perf_counter() - t
 
     rng = np.random.default_rng(5)
@@ -207,6 +240,7 @@ def main():
     ap.add_argument("--no-fp64-compare", action="store_true",
                     help="skip the one-step FP64-path measurement reported beside the mixed path")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying CUDA graphs")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=8.0)
@@ -236,7 +270,7 @@ def main():
 
     from sbpom_letkf_v2_b200.analysis import Analysis
     from sbpom_letkf_v2_b200.params import PREC_FP64, PREC_MIXED
-    from sbpom_letkf_v2_b200.synthetic import WORKLOADS, make_case
+    from sbpom_letkf_v2_b200.synthetic import WORKLOADS, make_case, pf_uniforms
 
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
@@ -251,10 +285,12 @@ def main():
     a3 = torch.empty_like(case.fcst3d)
     a2 = torch.empty_like(case.fcst2d)
     s = torch.cuda.current_stream()
+    pf = p.iswitch_da != 1
+    uni = pf_uniforms(wl.npoints, p.nmonte, p.nmem, p.rm, device=dev, seed=11 + rank) if pf else None
 
     def step():
         an.prepare_obs(case.obs)
-        an.da_main(case.grid, case.fcst3d, case.fcst2d, anal3d=a3, anal2d=a2, check=False)
+        an.da_main(case.grid, case.fcst3d, case.fcst2d, uniforms=uni, anal3d=a3, anal2d=a2, check=False)
 
     for _ in range(args.warmup):
         step()
@@ -265,6 +301,23 @@ def main():
             import torch.distributed as dist
             dist.barrier()
 
+    # one cycle = two CUDA graphs (observation bucketing, analysis), so the
+    # analysis kernel can be timed with events on this stream between them
+    g_prep = g_ana = None
+    if not args.no_graph:
+        cs = torch.cuda.Stream(device=dev)
+        cs.wait_stream(s)
+        g_prep, g_ana = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g_prep, stream=cs):
+            an.prepare_obs(case.obs)
+        with torch.cuda.graph(g_ana, stream=cs):
+            an.da_main(case.grid, case.fcst3d, case.fcst2d, uniforms=uni, anal3d=a3, anal2d=a2, check=False)
+        s.wait_stream(cs)
+        g_prep.replay()
+        g_ana.replay()
+        torch.cuda.synchronize()
+        an.raise_status()
+
     # ---- device-timed region: K steps, with the analysis kernel timed inside
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.synchronize()
@@ -274,10 +327,16 @@ def main():
     with Clocks(dev.index) as clk:
         t0.record(s)
         for i in range(args.steps):
-            an.prepare_obs(case.obs)
-            ev[i][0].record(s)
-            an.da_main(case.grid, case.fcst3d, case.fcst2d, anal3d=a3, anal2d=a2, check=False)
-            ev[i][1].record(s)
+            if g_prep is not None:
+                g_prep.replay()
+                ev[i][0].record(s)
+                g_ana.replay()
+                ev[i][1].record(s)
+            else:
+                an.prepare_obs(case.obs)
+                ev[i][0].record(s)
+                an.da_main(case.grid, case.fcst3d, case.fcst2d, uniforms=uni, anal3d=a3, anal2d=a2, check=False)
+                ev[i][1].record(s)
         t1.record(s)
         torch.cuda.synchronize()
     barrier()
@@ -303,7 +362,10 @@ def main():
         d_obs = {k: torch.empty_like(v, device=dev) for k, v in hobs.items()}
         d3 = torch.empty_like(case.fcst3d)
         d2 = torch.empty_like(case.fcst2d)
+        hu = uni.cpu().pin_memory() if pf else None
+        d_uni = torch.empty_like(uni) if pf else None
         h2d = sum(v.numel() * v.element_size() for v in hobs.values()) + hf3.numel() * 4 + hf2.numel() * 4
+        h2d += hu.numel() * 8 if pf else 0
         d2h = ha3.numel() * 4 + ha2.numel() * 4
 
         def e2e_step():
@@ -311,8 +373,10 @@ def main():
                 d_obs[k].copy_(v, non_blocking=True)
             d3.copy_(hf3, non_blocking=True)
             d2.copy_(hf2, non_blocking=True)
+            if pf:
+                d_uni.copy_(hu, non_blocking=True)
             an.prepare_obs(d_obs)
-            an.da_main(case.grid, d3, d2, anal3d=a3, anal2d=a2, check=False)
+            an.da_main(case.grid, d3, d2, uniforms=d_uni, anal3d=a3, anal2d=a2, check=False)
             ha3.copy_(a3, non_blocking=True)
             ha2.copy_(a2, non_blocking=True)
 
@@ -339,17 +403,18 @@ def main():
 
     # ---- the FP64 path on the same inputs (one warm-up, one timed step)
     fp64 = None
-    if prec == PREC_MIXED and not args.no_fp64_compare:
+    if prec == PREC_MIXED and not pf and not args.no_fp64_compare:
+        m3, m2 = a3.clone(), a2.clone()
         p64 = p.replace(precision=PREC_FP64)
         an.prepare_obs(case.obs)
-        an.da_main(case.grid, case.fcst3d, case.fcst2d, anal3d=a3, anal2d=a2, params=p64, check=False)
+        an.da_main(case.grid, case.fcst3d, case.fcst2d, uniforms=uni, anal3d=a3, anal2d=a2, params=p64, check=False)
         torch.cuda.synchronize()
         barrier()
         f0 = torch.cuda.Event(enable_timing=True)
         f1 = torch.cuda.Event(enable_timing=True)
         f0.record(s)
         an.prepare_obs(case.obs)
-        an.da_main(case.grid, case.fcst3d, case.fcst2d, anal3d=a3, anal2d=a2, params=p64, check=False)
+        an.da_main(case.grid, case.fcst3d, case.fcst2d, uniforms=uni, anal3d=a3, anal2d=a2, params=p64, check=False)
         f1.record(s)
         torch.cuda.synchronize()
         barrier()
@@ -360,34 +425,44 @@ def main():
             tt = torch.tensor([fms], device=dev, dtype=torch.float64)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             fms = float(tt[0])
-        fp64 = {"value": P * world / (fms / 1e3), "ms_per_step": fms, "mixed_over_fp64": fms / ms}
+        fp64 = {"value": P * world / (fms / 1e3), "ms_per_step": fms, "mixed_over_fp64": fms / ms,
+                "mixed_error": mean_spread_error(m3, m2, a3, a2)}
+        del m3, m2
 
+    state_gb = 2.0 * (case.fcst3d.numel() + case.fcst2d.numel()) * case.fcst3d.element_size() / 1e9
     if rank == 0:
         fl = algorithmic_flops(nobsl, p.nmem, p.nv3d, p.nv2d, p.nlev, case.nij1)
         f64 = _fp64_peak(dev)
-        achieved = fl["total"] / (kern_ms / 1e3) / 1e12
-        # DRAM bytes per launch: ncu capture of the same kernel on the 1/8 grid
-        # (profiles/analysis_mixed_workload1_scale8_full.md), 218.9 MB for
-        # 74,000 points, scaled by the points of this launch
-        traffic = 218.9e6 / 74000.0 * P if args.workload == 1 else None
-        roof = {"bound": "fp64", "achieved": achieved, "peak": f64["tflops"], "unit": "TFLOP/s",
-                "frac": achieved / f64["tflops"], "traffic": traffic, "kernel": "k_analysis",
-                "peak_source": f64["source"], "kernel_ms": kern_ms, "flops_per_launch": fl,
-                "note": "FP64 eigensolve bound; tensor pipe 0.46 % busy (ncu), traffic scaled from a 1/8-grid capture"}
+        peaks, src = _peaks()
+        if pf:
+            by = algorithmic_bytes(nobsl, p.nmem, p.nv3d, p.nv2d, p.nlev, case.nij1)
+            gbs = by["total"] / (kern_ms / 1e3) / 1e9
+            roof = {"bound": "hbm", "achieved": gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                    "frac": gbs / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None, "traffic": None,
+                    "kernel": "k_analysis (LPF weights + resampling gather)", "kernel_ms": kern_ms,
+                    "bytes_per_launch": by, "peak_source": src + " hbm_gbs (copy)",
+                    "note": "fused kernel: weights, nmonte draws and gather in one launch"}
+        else:
+            achieved = fl["total"] / (kern_ms / 1e3) / 1e12
+            roof = {"bound": "fp64", "achieved": achieved, "peak": f64["tflops"], "unit": "TFLOP/s",
+                    "frac": achieved / f64["tflops"], "traffic": None, "kernel": "k_analysis",
+                    "peak_source": f64["source"], "kernel_ms": kern_ms, "flops_per_launch": fl,
+                    "note": "FP64 eigensolve bound"}
         cpu = None
         if not args.no_cpu_baseline and world == 1:
-            cpu = cpu_baseline(case, p.replace(precision=PREC_FP64), seconds=15.0)
-        peaks, src = _peaks()
+            cpu = cpu_baseline(case, p.replace(precision=PREC_FP64), seconds=15.0, uniforms=uni)
         line = {"metric": METRIC, "value": value, "unit": "gridpoints/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64" if prec == PREC_FP64 else "bf16x2 gram (f32 acc) + f64 eig",
+                "vs_baseline": None,
+                "dtype": "f64" if (prec == PREC_FP64 or pf) else "bf16x3 gram (f32 acc) + f64 eig",
                 "data": "synthetic (seeded, generated in device memory)",
                 "config": {"workload": wl.name, "points": P, "nmem": p.nmem, "nobs": nobs,
                            "precision": args.precision, "nobsl_mean": float(nobsl.mean()),
-                           "nobsl_max": int(nobsl.max()), "l2": "inputs larger than L2 (7.7 GB state)",
+                           "nobsl_max": int(nobsl.max()), "nmonte": p.nmonte if pf else None,
+                           "l2": f"inputs larger than L2 ({state_gb:.2f} GB state read + written per step)",
                            "parallelism": f"replicas x{world}"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "fp64_path": fp64,
-                "gpu_launches": 6 * args.steps, "peaks_source": src,
+                "gpu_launches": 6 * args.steps, "graph": g_prep is not None, "peaks_source": src,
                 "hbm_peak_gbs": peaks.get("hbm_gbs")}
         print(json.dumps(line), flush=True)
     an.close()

@@ -55,8 +55,10 @@ extern "C" {
 #define SBLETKF_F64 1
 
 #define SBLETKF_PREC_FP64  0        /* every step in FP64 (plain path)          */
-#define SBLETKF_PREC_MIXED 1        /* Gram on tcgen05 BF16 hi/lo split, FP32
-                                       accumulate; eigensolve and transform FP64 */
+#define SBLETKF_PREC_MIXED 1        /* Gram on tcgen05 as a three-way BF16 split
+                                       (h+m+l) with FP32 accumulation (points
+                                       with > 12288 search-box candidates use
+                                       FP64); eigensolve and transform FP64 */
 
 #define SBLETKF_DA_LETKF 1          /* iswitch_da (common_setting.f90:65) */
 #define SBLETKF_DA_LPF   2

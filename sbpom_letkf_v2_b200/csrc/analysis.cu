@@ -25,14 +25,14 @@ namespace {
 
 // State of the tensor-core Gram pipeline of one CTA (uniform across threads).
 struct TcState {
-  uint32_t tbase;   // TMEM base: C1 at column 0, C2 at column KP
+  uint32_t tbase;   // TMEM base: the FP32 Gram accumulator, KP columns
   int uses[2];      // commits issued per operand stage
   int nchunk;
   int broken;       // a wait timed out: issue nothing more
 };
 
-// Stage `cnt` list entries starting at f as BF16 hi/lo operand tiles and issue
-// their two UMMAs per K-block (C1 += Zh^T Zh, C2 += Zh^T Zl).  Also
+// Stage `cnt` list entries starting at f as BF16 h/m/l operand tiles and issue
+// their six UMMAs per K-block into the Gram accumulator.  Also
 // accumulates b = sum w dep y (FP64) and, when do_pf, the PF log-likelihood.
 // Whole CTA; ends with the tiles handed to the tensor core.
 template <int KP>
@@ -44,7 +44,7 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
   const int s = st.nchunk & 1;
   float *stg = reinterpret_cast<float *>(S.u);  // [kKC][KP] FP32 rows
   unsigned char *tiles = reinterpret_cast<unsigned char *>(S.u) + PointSmem::tc_tiles_off(KP);
-  unsigned char *hi = tiles + s * kStageBytes, *lo = hi + kTileBytes;
+  unsigned char *stage = tiles + s * kStageBytes;
   float *sw = reinterpret_cast<float *>(S.cw);
   __shared__ int s_broken;
   if (tid == 0) {  // the stage's previous UMMAs must be done
@@ -83,20 +83,25 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
       const int o = g * 8 + i;
       z[i] = m < KP ? sw[o] * stg[o * KP + m] : 0.0f;
     }
-    store_split8(hi, lo, tile_off(m, g * 8), z);
+    store_split8(stage, tile_off(m, g * 8), z);
   }
   fence_async_smem();
   __syncthreads();
   if (tid == 0 && !st.broken) {
     fence_after_sync();
     const uint32_t idesc = idesc_bf16(kM, KP);
-    const uint32_t ah = smem_u32(hi), al = smem_u32(lo);
+    const uint32_t a0 = smem_u32(stage);
 #pragma unroll
     for (int kb = 0; kb < kKC / kKB; ++kb) {
-      const uint64_t da = sdesc(ah + kb * kBlockBytes), dl = sdesc(al + kb * kBlockBytes);
+      const uint64_t dh = sdesc(a0 + kb * kBlockBytes), dm = sdesc(a0 + kTileBytes + kb * kBlockBytes),
+                     dl = sdesc(a0 + 2 * kTileBytes + kb * kBlockBytes);
       const uint32_t acc = (st.nchunk > 0 || kb > 0) ? 1u : 0u;
-      mma_bf16(st.tbase, da, da, idesc, acc);
-      mma_bf16(st.tbase + KP, da, dl, idesc, acc);
+      mma_bf16(st.tbase, dh, dh, idesc, acc);  // H^T H
+      mma_bf16(st.tbase, dh, dm, idesc, 1u);   // H^T M
+      mma_bf16(st.tbase, dm, dh, idesc, 1u);   // M^T H
+      mma_bf16(st.tbase, dh, dl, idesc, 1u);   // H^T L
+      mma_bf16(st.tbase, dl, dh, idesc, 1u);   // L^T H
+      mma_bf16(st.tbase, dm, dm, idesc, 1u);   // M^T M
     }
     commit_to(&mbar[s]);
   }
@@ -104,8 +109,9 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
   st.nchunk++;
 }
 
-// Wait for every issued UMMA, then G = C1 + C2 + C2^T + alpha I into B (FP64,
-// column-major, stride ldb) and b into S.b.
+// Wait for every issued UMMA, then G + alpha I into B (FP64, column-major,
+// stride ldb; the lower triangle read from the accumulator and mirrored, so B
+// is exactly symmetric) and b into S.b.
 template <int KP>
 __device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint64_t *mbar, int k, double alpha,
                                           double bacc, int &bits) {
@@ -123,25 +129,17 @@ __device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint6
   double *B = S.u;
   const int q = wid & 3, half = wid >> 2, r = 32 * q + lane;
   const uint32_t trow = st.tbase + ((uint32_t)(32 * q) << 16);
-  float v1[16], v2[16];
-  for (int ch = half; ch < KP / 16; ch += 2) {  // pass 1: row r of C1 + C2
-    tmem_ld16(trow + 16 * ch, v1);
-    tmem_ld16(trow + KP + 16 * ch, v2);
+  float v[16];
+  for (int ch = half; ch < KP / 16; ch += 2) {  // row r, columns c <= r
+    tmem_ld16(trow + 16 * ch, v);
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int c = 16 * ch + i;
-      if (r < k && c < k) B[(long)c * S.ldb + r] = (double)v1[i] + (double)v2[i] + (r == c ? alpha : 0.0);
-    }
-  }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  for (int ch = half; ch < KP / 16; ch += 2) {  // pass 2: + C2^T, thread r owns column r
-    tmem_ld16(trow + KP + 16 * ch, v2);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int c = 16 * ch + i;
-      if (r < k && c < k) B[(long)r * S.ldb + c] += (double)v2[i];
+      if (r < k && c <= r) {
+        const double g = (double)v[i] + (r == c ? alpha : 0.0);
+        B[(long)c * S.ldb + r] = g;
+        B[(long)r * S.ldb + c] = g;
+      }
     }
   }
   if (tid < k) S.b[tid] = bacc;
@@ -170,14 +168,14 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ uint64_t s_mbar[2];
   __shared__ uint32_t s_tmem;
   int bits = 0;
-  constexpr uint32_t kTmemCols = (2 * KP <= 64) ? 64 : (2 * KP <= 128) ? 128 : 256;
-  const bool use_tc = MIXED && do_gram;
+  constexpr uint32_t kTmemCols = (KP <= 32) ? 32 : (KP <= 64) ? 64 : 128;
+  const bool tc_on = MIXED && do_gram;  // TMEM and barriers held by this CTA
   TcState tcs;
   tcs.uses[0] = tcs.uses[1] = 0;
   tcs.nchunk = 0;
   tcs.tbase = 0;
   tcs.broken = 0;
-  if (use_tc) {
+  if (tc_on) {
     // after a tensor-core wait has timed out anywhere in the launch, later
     // CTAs return at once (the status word already carries the error)
     __shared__ int s_abort;
@@ -215,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   __syncthreads();
   bits |= sh[5];
-  if (use_tc) {
+  if (tc_on) {
     tc::fence_after_sync();
     tcs.tbase = s_tmem;
   }
@@ -250,6 +248,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
   }
   const int ncand = S.rowpref[nrows];
+  // FP32 accumulation in tensor memory is accurate to ~eps32 sqrt(n/16) |G|;
+  // points whose search box holds more candidates take the FP64 Gram
+  const bool use_tc = tc_on && ncand <= tc::kMaxCand;
 
   // ---- streaming local-obs selection + accumulation (obs order preserved).
   // Rows are consumed on the fly once nobsl exceeds the dual limit; below it
@@ -560,8 +561,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (v < p.nv3d) a3[(((long)v * k + m) * nlev + kl) * nij1 + i] = (ST)a;
     else a2[((long)(v - p.nv3d) * k + m) * nij1 + i] = (ST)a;
   }
-  if (use_tc && (bits & SBLETKF_ERR_TIMEOUT)) atomicOr(status, SBLETKF_ERR_TIMEOUT);
-  if (use_tc) {  // every UMMA was waited for in tc_finish (or never issued)
+  if (tc_on && (bits & SBLETKF_ERR_TIMEOUT)) atomicOr(status, SBLETKF_ERR_TIMEOUT);
+  if (tc_on) {  // every UMMA was waited for in tc_finish (or never issued)
     tc::fence_before_sync();
     __syncthreads();
     if ((tid >> 5) == 0) {

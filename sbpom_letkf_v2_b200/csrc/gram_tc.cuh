@@ -1,12 +1,15 @@
 // gram_tc.cuh -- the local Gram Y^T diag(rloc/rdiag) Y on the 5th-generation
 // tensor cores (tcgen05, sm_100a), split-precision BF16.
 //
-// With z_o = sqrt(rloc_o/rdiag_o) y_o the Gram is G = Z^T Z.  Each row is split
-// into z = hi + lo with hi = bf16(z), lo = bf16(z - hi) (16 significant bits),
-// and G ~= Zh^T Zh + Zh^T Zl + Zl^T Zh = C1 + C2 + C2^T: two UMMAs per K-block
-// accumulate C1 and C2 in FP32 in tensor memory; the dropped Zl^T Zl term is
-// below 2^-16 of G.  (common_letkf.f90:93-122 computes the same Gram with
-// sgemm/dgemm.)
+// With z_o = sqrt(rloc_o/rdiag_o) y_o the Gram is G = Z^T Z.  Each FP32 row is
+// split three ways, z = h + m + l with h = bf16(z), m = bf16(z - h),
+// l = bf16(z - h - m) (24 significant bits, all of FP32), and
+//   G ~= H^T H + H^T M + M^T H + H^T L + L^T H + M^T M,
+// six UMMAs per K-block into one FP32 accumulator in tensor memory; the
+// dropped terms (M^T L, L^T M, L^T L) are below 2^-24 of G, so the Gram is as
+// accurate as FP32 accumulation allows.  Transposed pairs are separate UMMAs
+// (A and B swapped), so the accumulator needs no transpose.
+// (common_letkf.f90:93-122 computes the same Gram with sgemm/dgemm.)
 //
 // Operand tile: rows = members (M = 128, zero-padded), K = observations, in the
 // K-major canonical layout without swizzle: 8x8 "core matrices" of 8 rows x 16
@@ -27,9 +30,14 @@ constexpr int kM = 128;            // UMMA M (members, zero padded)
 constexpr int kKC = 64;            // observations per staged chunk (4 K-blocks)
 constexpr int kKB = 16;            // UMMA K for kind::f16
 constexpr int kBlockBytes = kM * kKB * 2;             // one 16-wide K block, 4096 B
-constexpr int kTileBytes = kBlockBytes * (kKC / kKB);  // one chunk, hi or lo: 16 KB
-constexpr int kStageBytes = 2 * kTileBytes;            // hi + lo
+constexpr int kTileBytes = kBlockBytes * (kKC / kKB);  // one chunk of one split part: 16 KB
+constexpr int kSplit = 3;                              // h, m, l
+constexpr int kStageBytes = kSplit * kTileBytes;
 constexpr unsigned kWaitLimit = 1u << 20;              // bounded mbarrier polls
+// Largest search-box candidate count whose Gram goes to the tensor cores: the
+// FP32 accumulator's rounding grows like eps32 sqrt(n/16) |G|, which must stay
+// well below alpha = (k-1)/rho for the eigensolve; denser points use FP64.
+constexpr int kMaxCand = 12288;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -116,21 +124,28 @@ __device__ __forceinline__ uint32_t tile_off(int row, int k) {
   return (uint32_t)((k >> 4) * kBlockBytes + (row >> 3) * 256 + ((k >> 3) & 1) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-// Split 8 FP32 values into BF16 hi / lo and store them as two 16-byte rows of
-// the hi and lo tiles.
-__device__ __forceinline__ void store_split8(unsigned char *hi_tile, unsigned char *lo_tile, uint32_t off,
-                                             const float *z) {
-  uint32_t h[4], l[4];
+// Split 8 FP32 values into BF16 h / m / l and store them as 16-byte rows of
+// the three tiles (tile j at t + j * kTileBytes).
+__device__ __forceinline__ void store_split8(unsigned char *t, uint32_t off, const float *z) {
+  uint32_t h[4], m[4], l[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const __nv_bfloat16 h0 = __float2bfloat16_rn(z[2 * i]), h1 = __float2bfloat16_rn(z[2 * i + 1]);
-    const __nv_bfloat16 l0 = __float2bfloat16_rn(z[2 * i] - __bfloat162float(h0));
-    const __nv_bfloat16 l1 = __float2bfloat16_rn(z[2 * i + 1] - __bfloat162float(h1));
-    h[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-    l[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    __nv_bfloat16 a[2], b[2], c[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const float x = z[2 * i + u];
+      a[u] = __float2bfloat16_rn(x);
+      const float r1 = x - __bfloat162float(a[u]);
+      b[u] = __float2bfloat16_rn(r1);
+      c[u] = __float2bfloat16_rn(r1 - __bfloat162float(b[u]));
+    }
+    h[i] = (uint32_t)__bfloat16_as_ushort(a[0]) | ((uint32_t)__bfloat16_as_ushort(a[1]) << 16);
+    m[i] = (uint32_t)__bfloat16_as_ushort(b[0]) | ((uint32_t)__bfloat16_as_ushort(b[1]) << 16);
+    l[i] = (uint32_t)__bfloat16_as_ushort(c[0]) | ((uint32_t)__bfloat16_as_ushort(c[1]) << 16);
   }
-  *reinterpret_cast<uint4 *>(hi_tile + off) = make_uint4(h[0], h[1], h[2], h[3]);
-  *reinterpret_cast<uint4 *>(lo_tile + off) = make_uint4(l[0], l[1], l[2], l[3]);
+  *reinterpret_cast<uint4 *>(t + off) = make_uint4(h[0], h[1], h[2], h[3]);
+  *reinterpret_cast<uint4 *>(t + kTileBytes + off) = make_uint4(m[0], m[1], m[2], m[3]);
+  *reinterpret_cast<uint4 *>(t + 2 * kTileBytes + off) = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
 }  // namespace tc

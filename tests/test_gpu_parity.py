@@ -141,7 +141,7 @@ def test_bad_obs_cell_raises(cuda):
         run_gpu(case.params, g, ob, f3, f2)
 
 
-# ---- mixed precision: tcgen05 BF16 hi/lo Gram, FP64 eigensolve and transform
+# ---- mixed precision: tcgen05 three-way BF16 split Gram, FP64 eigensolve and transform
 TOL_MIXED = 1e-4   # relative error of analysis mean and spread vs the FP64 oracle
 
 
@@ -174,5 +174,20 @@ def test_mixed_lpfgm_within_1e4(cuda):
     uni = pf_uniforms(P, 4, 48, RM_SR).numpy()
     ref = cref.da_main(case.params, g, ob, f3, f2, uniforms=uni, rsize=8)
     r = run_gpu(case.params.replace(precision=1), g, ob, f3, f2, uni=uni)
+    em, es = _mean_spread_err(r["anal3d"], ref["anal3d"])
+    assert em <= TOL_MIXED and es <= TOL_MIXED
+
+
+def test_mixed_dense_points_route_to_fp64_gram(cuda):
+    """Points whose search box holds more than 12288 candidates take the FP64
+    Gram inside the mixed kernel (FP32 accumulation over that many
+    observations would no longer keep A = G + alpha I positive definite)."""
+    wl = WORKLOADS[0].scaled(nlon=20, nlat=16, nlev=3, nmem=64, n_sst=14000, n_ssh=0, n_prof=4, seed=811)
+    case = make_case(wl, cov_infl_mul=1.1)
+    g, ob, f3, f2 = _np(case)
+    ref = cref.da_main(case.params, g, ob, f3, f2, rsize=8)
+    r = run_gpu(case.params.replace(precision=1), g, ob, f3, f2)
+    assert (r["status"] == 0).all()
+    assert r["nobsl"].max() > 12288   # every search box here holds 14,040 candidates
     em, es = _mean_spread_err(r["anal3d"], ref["anal3d"])
     assert em <= TOL_MIXED and es <= TOL_MIXED
