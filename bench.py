@@ -203,6 +203,17 @@ def scaled_workload(wl, s: int):
                      name=wl.name + f" (1/{s} grid)")
 
 
+def config_of(wl, p, args, world) -> dict:
+    """The workload description shared by both arms' JSON lines."""
+    state_gb = 2.0 * 4.0 * wl.nmem * wl.nlon * wl.nlat * (4 * wl.nlev + 1) / 1e9
+    pf = p.iswitch_da != 1
+    return {"workload": wl.name, "points": wl.npoints, "nmem": p.nmem, "nobs": wl.nobs,
+            "precision": args.precision if not pf else "fp64", "nmonte": p.nmonte if pf else None,
+            "l2": (f"inputs larger than L2 ({state_gb:.2f} GB FP32 state read + written per step)"
+                   if state_gb > 0.126 else f"inputs fit in L2 ({state_gb:.3f} GB), not flushed"),
+            "parallelism": f"replicas x{world}"}
+
+
 def reference_arm(args, rank, world):
     """--impl reference: the CPU restatement timed per step on a bounded sample."""
     from sbpom_letkf_v2_b200.synthetic import WORKLOADS, make_case
@@ -212,9 +223,13 @@ def reference_arm(args, rank, world):
     wl = scaled_workload(WORKLOADS[args.workload], args.scale)
     case = make_case(wl, device=dev, seed=wl.seed)
     p = case.params.replace(precision=0)
+    uni = None
+    if p.iswitch_da != 1:
+        from sbpom_letkf_v2_b200.synthetic import pf_uniforms
+        uni = pf_uniforms(wl.npoints, p.nmonte, p.nmem, p.rm, device=dev, seed=11)
     vals = []
     for s in range(args.warmup + args.steps):
-        r = cpu_baseline(case, p, seconds=args.ref_seconds)
+        r = cpu_baseline(case, p, seconds=args.ref_seconds, uniforms=uni)
         if s >= args.warmup:
             vals.append(r["value"])
     v = float(np.mean(vals))
@@ -222,8 +237,7 @@ def reference_arm(args, rank, world):
             "warmup": args.warmup, "ms_per_step": 1e3 * wl.npoints / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": wl.name, "points": wl.npoints, "nmem": wl.nmem, "nobs": wl.nobs,
-                       "l2": "inputs larger than L2"},
+            "config": config_of(wl, case.params, args, world),
             "cpu_baseline": {"value": v, "unit": "gridpoints/s", "cores": r["cores"], "kind": "port",
                              "sample": r["sample"]},
             "e2e": {"value": v, "unit": "gridpoints/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -429,7 +443,6 @@ def main():
                 "mixed_error": mean_spread_error(m3, m2, a3, a2)}
         del m3, m2
 
-    state_gb = 2.0 * (case.fcst3d.numel() + case.fcst2d.numel()) * case.fcst3d.element_size() / 1e9
     if rank == 0:
         fl = algorithmic_flops(nobsl, p.nmem, p.nv3d, p.nv2d, p.nlev, case.nij1)
         f64 = _fp64_peak(dev)
@@ -456,11 +469,8 @@ def main():
                 "vs_baseline": None,
                 "dtype": "f64" if (prec == PREC_FP64 or pf) else "bf16x3 gram (f32 acc) + f64 eig",
                 "data": "synthetic (seeded, generated in device memory)",
-                "config": {"workload": wl.name, "points": P, "nmem": p.nmem, "nobs": nobs,
-                           "precision": args.precision, "nobsl_mean": float(nobsl.mean()),
-                           "nobsl_max": int(nobsl.max()), "nmonte": p.nmonte if pf else None,
-                           "l2": f"inputs larger than L2 ({state_gb:.2f} GB state read + written per step)",
-                           "parallelism": f"replicas x{world}"},
+                "config": config_of(wl, p, args, world),
+                "nobsl": {"mean": float(nobsl.mean()), "max": int(nobsl.max()), "zero_frac": float((nobsl == 0).mean())},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "fp64_path": fp64,
                 "gpu_launches": 6 * args.steps, "graph": g_prep is not None, "peaks_source": src,
                 "hbm_peak_gbs": peaks.get("hbm_gbs")}

@@ -25,14 +25,56 @@ namespace {
 
 // State of the tensor-core Gram pipeline of one CTA (uniform across threads).
 struct TcState {
-  uint32_t tbase;   // TMEM base: the FP32 Gram accumulator, KP columns
+  uint32_t tbase;   // TMEM base: sum hi, sum lo, chunk accumulators 0 and 1 (KP columns each)
   int uses[2];      // commits issued per operand stage
   int nchunk;
+  int nflushed;     // chunks added into the running sum
   int broken;       // a wait timed out: issue nothing more
 };
 
+// Add the chunk accumulator of stage s into the running double-FP32 sum with
+// Knuth's TwoSum (hi + c = s_ + e exactly; lo += e).  Whole CTA: warp w owns
+// TMEM lanes 32 (w % 4) .. +31 and half w / 4 of the 16-column groups.
+template <int KP>
+__device__ __forceinline__ void tc_flush(TcState &st, int s) {
+  using namespace tc;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  (void)lane;
+  const int q = wid & 3, half = wid >> 2;
+  const uint32_t trow = st.tbase + ((uint32_t)(32 * q) << 16);
+  const uint32_t cc = (uint32_t)((2 + s) * KP);
+  const bool first = st.nflushed == 0;
+  float c[16], h[16], l[16];
+  for (int ch = half; ch < KP / 16; ch += 2) {
+    tmem_ld16(trow + cc + 16 * ch, c);
+    if (first) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        h[i] = c[i];
+        l[i] = 0.0f;
+      }
+    } else {
+      tmem_ld16(trow + 16 * ch, h);
+      tmem_ld16(trow + KP + 16 * ch, l);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const float t = __fadd_rn(h[i], c[i]);
+        const float bv = __fsub_rn(t, h[i]);
+        const float e = __fadd_rn(__fsub_rn(h[i], __fsub_rn(t, bv)), __fsub_rn(c[i], bv));
+        h[i] = t;
+        l[i] = __fadd_rn(l[i], e);
+      }
+    }
+    tmem_st16(trow + 16 * ch, h);
+    tmem_st16(trow + KP + 16 * ch, l);
+  }
+  tmem_wait_st();
+  st.nflushed++;
+}
+
 // Stage `cnt` list entries starting at f as BF16 h/m/l operand tiles and issue
-// their six UMMAs per K-block into the Gram accumulator.  Also
+// their six UMMAs per K-block into the stage's chunk accumulator, after adding
+// that accumulator's previous chunk into the running sum.  Also
 // accumulates b = sum w dep y (FP64) and, when do_pf, the PF log-likelihood.
 // Whole CTA; ends with the tiles handed to the tensor core.
 template <int KP>
@@ -65,6 +107,11 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
   if (tid < kKC) sw[tid] = tid < cnt ? (float)sqrt(S.lw[f + tid]) : 0.0f;
   __syncthreads();
   st.broken = s_broken;
+  if (!st.broken && st.uses[s] > 0) {  // the chunk two back is complete: add it to the sum
+    fence_after_sync();
+    tc_flush<KP>(st, s);
+    fence_before_sync();
+  }
   if (tid < KP)
     for (int cc = 0; cc < cnt; ++cc) bacc = fma(S.lwd[f + cc], (double)stg[cc * KP + tid], bacc);
   if (do_pf && tid < k) {
@@ -95,13 +142,14 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
     for (int kb = 0; kb < kKC / kKB; ++kb) {
       const uint64_t dh = sdesc(a0 + kb * kBlockBytes), dm = sdesc(a0 + kTileBytes + kb * kBlockBytes),
                      dl = sdesc(a0 + 2 * kTileBytes + kb * kBlockBytes);
-      const uint32_t acc = (st.nchunk > 0 || kb > 0) ? 1u : 0u;
-      mma_bf16(st.tbase, dh, dh, idesc, acc);  // H^T H
-      mma_bf16(st.tbase, dh, dm, idesc, 1u);   // H^T M
-      mma_bf16(st.tbase, dm, dh, idesc, 1u);   // M^T H
-      mma_bf16(st.tbase, dh, dl, idesc, 1u);   // H^T L
-      mma_bf16(st.tbase, dl, dh, idesc, 1u);   // L^T H
-      mma_bf16(st.tbase, dm, dm, idesc, 1u);   // M^T M
+      const uint32_t acc = kb > 0 ? 1u : 0u;   // each chunk starts a fresh accumulator
+      const uint32_t d = st.tbase + (uint32_t)((2 + s) * KP);
+      mma_bf16(d, dh, dh, idesc, acc);  // H^T H
+      mma_bf16(d, dh, dm, idesc, 1u);   // H^T M
+      mma_bf16(d, dm, dh, idesc, 1u);   // M^T H
+      mma_bf16(d, dh, dl, idesc, 1u);   // H^T L
+      mma_bf16(d, dl, dh, idesc, 1u);   // L^T H
+      mma_bf16(d, dm, dm, idesc, 1u);   // M^T M
     }
     commit_to(&mbar[s]);
   }
@@ -109,34 +157,42 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
   st.nchunk++;
 }
 
-// Wait for every issued UMMA, then G + alpha I into B (FP64, column-major,
-// stride ldb; the lower triangle read from the accumulator and mirrored, so B
-// is exactly symmetric) and b into S.b.
+// Wait for every issued UMMA, add the last chunks into the running sum, then
+// G + alpha I = hi + lo + alpha I into B (FP64, column-major, stride ldb; the
+// lower triangle read and mirrored, so B is exactly symmetric) and b into S.b.
 template <int KP>
 __device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint64_t *mbar, int k, double alpha,
                                           double bacc, int &bits) {
   using namespace tc;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  __shared__ int s_brk;
   if (tid == 0) {
+    int brk = st.broken;
     for (int s = 0; s < 2; ++s)
-      if (!st.broken && st.uses[s] > 0 && !mbar_wait(&mbar[s], (uint32_t)((st.uses[s] - 1) & 1))) {
+      if (!brk && st.uses[s] > 0 && !mbar_wait(&mbar[s], (uint32_t)((st.uses[s] - 1) & 1))) {
         bits |= SBLETKF_ERR_TIMEOUT;
-        st.broken = 1;
+        brk = 1;
       }
+    s_brk = brk;
   }
   __syncthreads();
+  st.broken = s_brk;
   fence_after_sync();
+  if (!st.broken)
+    for (int t = st.nchunk - 2; t < st.nchunk; ++t)
+      if (t >= 0) tc_flush<KP>(st, t & 1);
   double *B = S.u;
   const int q = wid & 3, half = wid >> 2, r = 32 * q + lane;
   const uint32_t trow = st.tbase + ((uint32_t)(32 * q) << 16);
-  float v[16];
+  float vh[16], vl[16];
   for (int ch = half; ch < KP / 16; ch += 2) {  // row r, columns c <= r
-    tmem_ld16(trow + 16 * ch, v);
+    tmem_ld16(trow + 16 * ch, vh);
+    tmem_ld16(trow + KP + 16 * ch, vl);
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int c = 16 * ch + i;
       if (r < k && c <= r) {
-        const double g = (double)v[i] + (r == c ? alpha : 0.0);
+        const double g = (double)vh[i] + (double)vl[i] + (r == c ? alpha : 0.0);
         B[(long)c * S.ldb + r] = g;
         B[(long)r * S.ldb + c] = g;
       }
@@ -168,11 +224,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ uint64_t s_mbar[2];
   __shared__ uint32_t s_tmem;
   int bits = 0;
-  constexpr uint32_t kTmemCols = (KP <= 32) ? 32 : (KP <= 64) ? 64 : 128;
+  constexpr uint32_t kTmemCols = (4 * KP <= 128) ? 128 : (4 * KP <= 256) ? 256 : 512;
   const bool tc_on = MIXED && do_gram;  // TMEM and barriers held by this CTA
   TcState tcs;
   tcs.uses[0] = tcs.uses[1] = 0;
   tcs.nchunk = 0;
+  tcs.nflushed = 0;
   tcs.tbase = 0;
   tcs.broken = 0;
   if (tc_on) {

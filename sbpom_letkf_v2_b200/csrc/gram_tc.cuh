@@ -5,10 +5,14 @@
 // split three ways, z = h + m + l with h = bf16(z), m = bf16(z - h),
 // l = bf16(z - h - m) (24 significant bits, all of FP32), and
 //   G ~= H^T H + H^T M + M^T H + H^T L + L^T H + M^T M,
-// six UMMAs per K-block into one FP32 accumulator in tensor memory; the
-// dropped terms (M^T L, L^T M, L^T L) are below 2^-24 of G, so the Gram is as
-// accurate as FP32 accumulation allows.  Transposed pairs are separate UMMAs
-// (A and B swapped), so the accumulator needs no transpose.
+// six UMMAs per K-block into an FP32 chunk accumulator in tensor memory; the
+// dropped terms (M^T L, L^T M, L^T L) are below 2^-24 of G.  Transposed pairs
+// are separate UMMAs (A and B swapped), so the accumulator needs no transpose.
+// Each chunk (64 observations) has its own accumulator, which the CTA adds
+// into a running double-FP32 sum (hi + lo, error-free TwoSum) also held in
+// tensor memory, so FP32 rounding stays at the scale of one chunk rather than
+// growing with nobsl.  Tensor-memory columns: sum hi [0,KP), sum lo [KP,2KP),
+// chunk accumulators of the two operand stages [2KP,3KP) and [3KP,4KP).
 // (common_letkf.f90:93-122 computes the same Gram with sgemm/dgemm.)
 //
 // Operand tile: rows = members (M = 128, zero-padded), K = observations, in the
@@ -118,6 +122,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+
+// Store 16 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float *v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])), "r"(__float_as_uint(v[3])),
+      "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])), "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])),
+      "r"(__float_as_uint(v[8])), "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])),
+      "r"(__float_as_uint(v[11])), "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])),
+      "r"(__float_as_uint(v[14])), "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // Byte offset of (row, k) inside one chunk tile (k in [0, kKC)).
 __device__ __forceinline__ uint32_t tile_off(int row, int k) {

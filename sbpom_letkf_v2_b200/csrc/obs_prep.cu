@@ -76,7 +76,7 @@ __global__ void k_gather(int nobs, int nmem, int ldh, const int32_t *__restrict_
                          const double *__restrict__ dep, const HT *__restrict__ hdxf, int32_t *__restrict__ s_elm,
                          double *__restrict__ s_lon, double *__restrict__ s_lat, double *__restrict__ s_lev,
                          double *__restrict__ s_rdiag, double *__restrict__ s_dep, double *__restrict__ h64,
-                         float *__restrict__ h32) {
+                         float *__restrict__ h32, int *__restrict__ status) {
   const int lane = threadIdx.x & 31;
   const long long s = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (s >= nobs) return;
@@ -97,12 +97,20 @@ __global__ void k_gather(int nobs, int nmem, int ldh, const int32_t *__restrict_
     s_lev[s] = lev[o];
     s_rdiag[s] = err[o] * err[o];  // rdiag = obserr**2 (common_da.f90:280)
     s_dep[s] = dep[o];
+    // an observation the analysis cannot use: non-finite values or err <= 0
+    // (rdiag divides the localization weight, common_da.f90:280-287)
+    if (!isfinite(lon[o]) || !isfinite(lat[o]) || !isfinite(lev[o]) || !isfinite(dep[o]) || !(err[o] > 0.0) ||
+        !isfinite(err[o]))
+      atomicOr(status, SBLETKF_ERR_NONFINITE);
   }
+  bool bad = false;
   for (int m = lane; m < ldh; m += 32) {
     double v = m < nmem ? (double)hdxf[(long long)m * nobs + o] : 0.0;
+    bad |= !isfinite(v);
     row64[m] = v;
     row32[m] = (float)v;
   }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(status, SBLETKF_ERR_NONFINITE);
 }
 
 }  // namespace
@@ -128,12 +136,12 @@ int launch_prepare_obs(sbletkf_workspace *ws, const sbletkf_params *p, const sbl
       k_gather<double><<<nb, tb, 0, s>>>(nobs, p->nmem, ws->ldh, ws->d_cellstart + ncell, ws->d_perm, obs->elm,
                                          obs->lon, obs->lat, obs->lev, obs->err, obs->dep,
                                          (const double *)obs->hdxf, ws->d_elm, ws->d_lon, ws->d_lat, ws->d_lev,
-                                         ws->d_rdiag, ws->d_dep, ws->d_hdxf64, ws->d_hdxf32);
+                                         ws->d_rdiag, ws->d_dep, ws->d_hdxf64, ws->d_hdxf32, ws->d_status);
     else
       k_gather<float><<<nb, tb, 0, s>>>(nobs, p->nmem, ws->ldh, ws->d_cellstart + ncell, ws->d_perm, obs->elm,
                                         obs->lon, obs->lat, obs->lev, obs->err, obs->dep,
                                         (const float *)obs->hdxf, ws->d_elm, ws->d_lon, ws->d_lat, ws->d_lev,
-                                        ws->d_rdiag, ws->d_dep, ws->d_hdxf64, ws->d_hdxf32);
+                                        ws->d_rdiag, ws->d_dep, ws->d_hdxf64, ws->d_hdxf32, ws->d_status);
   }
   return cuda_status(cudaGetLastError());
 }
