@@ -358,13 +358,14 @@ static __device__ __forceinline__ int jacobi_sweeps(double *B, int n, int ldb, d
     __syncthreads();
     if (!rot) break;
   }
+  if (threadIdx.x == 0) flag[3] = sweep;  // sweeps run (diagnostics)
   __syncthreads();
   return sweep >= maxsw ? SBLETKF_ERR_EIG_NOCONV : 0;
 }
 
 // Eigenpairs of the SPD matrix in B: eigenvectors replace B's columns and
 // lam[] receives the eigenvalues.  vec: n doubles, perm: n ints of scratch;
-// flag: >= 3 shared ints.  Returns status bits.
+// flag: >= 4 shared ints (flag[3] = sweeps run).  Returns status bits.
 template <int EMAX>
 static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, double tol, int maxsw, double *lam,
                                                  int *flag, int *perm, double *vec) {
