@@ -85,7 +85,9 @@ typedef struct sbletkf_params {
   int32_t id_z_obs;    /* SSH element id              (:59)                   */
   int32_t precision;   /* SBLETKF_PREC_*                                      */
   int32_t max_sweeps;  /* Jacobi sweep cap (status flag when reached)         */
-  int32_t reserved_i[3];
+  int32_t iv3d_u;      /* 0-based index of zonal velocity among 3D vars (:42) */
+  int32_t iv3d_v;      /* 0-based index of meridional velocity (:43)         */
+  int32_t iv2d_z;      /* 0-based index of SSH among 2D vars (:46)           */
   double cov_infl_mul; /* multiplicative inflation rho (:71)                  */
   double cov_infl_gm;  /* LPFGM inflation            (:89)                    */
   double alpha_rtpp;   /* (:74)                                               */
@@ -202,6 +204,53 @@ int sbletkf_analysis_noalloc(const sbletkf_params *p, const sbletkf_grid *grid, 
                              const void *fcst3d, const void *fcst2d, void *anal3d, void *anal2d,
                              int32_t state_dtype, const double *uniforms, int32_t *point_status,
                              void *stream);
+
+/* ---- observation-space preprocessing (set_obs) --------------------------- */
+/* Raw observations: what read_obs delivers (common_io.f90:1113-1210). */
+typedef struct sbletkf_obs_in {
+  int32_t nobs, reserved;
+  const int32_t *elm;               /* element id (common_setting.f90:56-60)  */
+  const double *lon, *lat;          /* degrees                                */
+  const double *lev;                /* depth [m], <= 0 below the surface      */
+  const double *dat;                /* observed value                         */
+  const double *err;                /* prescribed error standard deviation    */
+} sbletkf_obs_in;
+
+/* Per-observation results; any pointer may be NULL (not written). */
+typedef struct sbletkf_obs_out {
+  int32_t *idx, *idy;               /* cell indices, 1-based, 0 outside       */
+  int32_t *qc;                      /* 1 usable, 0 undef or rejected          */
+  double *hxmean, *hxsprd;          /* ensemble mean / spread of H(x)         */
+  double *dep;                      /* innovation dat - hxmean                */
+  double *err;                      /* error std after AOEI                   */
+  double *hdxf;                     /* [nmem][nobs] H(x_m) - hxmean           */
+} sbletkf_obs_out;
+
+#define SBLETKF_OBSOP_GROSS_QC 1    /* LGE_IO: gross-error check (only with AOEI off) */
+#define SBLETKF_OBSOP_AOEI     2    /* adaptive observation error inflation   */
+
+/* Observation operator and departures: set_obs (common_obs.f90:24-265,
+ * 380-399) with Trans_XtoY (common.f90:391-500) and obs_id_uniform
+ * (common.f90:112-168) for every member, on the device.  Grid arrays are
+ * global, [nlat*nlon] with longitude fastest (lon, lat, fsm = sea mask,
+ * 0 on land) and depth [nlev][nlat*nlon]; state3d [nv3d][nmem][nlev][nlat*nlon],
+ * state2d [nv2d][nmem][nlat*nlon] (state_dtype).  Undef results are NaN.
+ * stats (optional, [(nv3d+nv2d)*3], added to): count, sum dep, sum dep^2 of
+ * the qc = 1 observations per variable (monit_dep, common.f90:602-675).
+ * Needs nlev >= 6 (the Akima stencil). */
+int sbletkf_obs_operator(const sbletkf_params *p, const double *glon, const double *glat, const double *gfsm,
+                         const double *gdepth, const void *state3d, const void *state2d, int32_t state_dtype,
+                         const sbletkf_obs_in *obs, int32_t flags, const sbletkf_obs_out *out, double *stats,
+                         void *stream);
+
+/* Ensemble mean and spread (k-1) of a state, per variable, level and point
+ * (ensemble_mesp, common.f90:505-596): state3d [nv3d][nmem][nlev][nij1] ->
+ * mean3d / sprd3d [nv3d][nlev][nij1], state2d [nv2d][nmem][nij1] -> mean2d /
+ * sprd2d [nv2d][nij1], all in state_dtype; the spread pointers may be NULL.
+ * Spread is NaN (the reference's undef) for nmem = 1. */
+int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const void *state3d, const void *state2d,
+                                 int32_t state_dtype, void *mean3d, void *sprd3d, void *mean2d, void *sprd2d,
+                                 void *stream);
 
 /* Vector-Jacobian product of the LETKF analysis (iswitch_da = 1, with RTPP,
  * RTPS and the T/S round-off): given dJ/d anal3d and dJ/d anal2d (same layouts

@@ -27,7 +27,8 @@ _NAMES = {ERR_ARG: "bad argument", ERR_CUDA: "CUDA error", ERR_WORKSPACE: "works
 #: every symbol include/sbletkf.h declares
 EXPORTS = ("sbletkf_abi_version", "sbletkf_workspace_create", "sbletkf_workspace_destroy",
            "sbletkf_prepare_obs", "sbletkf_analysis", "sbletkf_count_nobsl", "sbletkf_get_status",
-           "sbletkf_core_batched", "sbletkf_backward", "sbletkf_analysis_noalloc")
+           "sbletkf_core_batched", "sbletkf_backward", "sbletkf_analysis_noalloc",
+           "sbletkf_obs_operator", "sbletkf_ensemble_mean_spread")
 NOALLOC_MAX_OBS, NOALLOC_MAX_CELLS = 8192, 65536
 
 
@@ -43,6 +44,15 @@ class SBLETKFError(RuntimeError):
 class CGrid(ctypes.Structure):
     _fields_ = [("nij1", ctypes.c_int32), ("reserved", ctypes.c_int32)] + [
         (n, ctypes.c_void_p) for n in ("lon1", "lat1", "ri1", "rj1", "dlon1", "dlat1", "phi1", "depth1")]
+
+
+class CObsIn(ctypes.Structure):
+    _fields_ = [("nobs", ctypes.c_int32), ("reserved", ctypes.c_int32)] + [
+        (n, ctypes.c_void_p) for n in ("elm", "lon", "lat", "lev", "dat", "err")]
+
+
+class CObsOut(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in ("idx", "idy", "qc", "hxmean", "hxsprd", "dep", "err", "hdxf")]
 
 
 class CObs(ctypes.Structure):
@@ -75,6 +85,9 @@ def load(path: str = LIB_PATH):
                              ctypes.c_int),
         "sbletkf_analysis_noalloc": ([pp, ctypes.POINTER(CGrid), ctypes.POINTER(CObs), vp, vp, vp, vp, i32, vp,
                                       vp, vp], ctypes.c_int),
+        "sbletkf_obs_operator": ([pp, vp, vp, vp, vp, vp, vp, i32, ctypes.POINTER(CObsIn), i32,
+                                  ctypes.POINTER(CObsOut), vp, vp], ctypes.c_int),
+        "sbletkf_ensemble_mean_spread": ([pp, i32, vp, vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -234,3 +234,25 @@ def core_batched(params: LETKFParams, nobsl, hdxf, rdiag, rloc, dep, uniforms=No
                                         _stream_ptr(stream)), "core_batched")
     torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
     return wvec, wmat
+
+
+def ensemble_mean_spread(params: LETKFParams, state3d: torch.Tensor, state2d: torch.Tensor, stream=None):
+    """Ensemble mean and spread of a state (ensemble_mesp, common.f90:505-596):
+    [nv3d][nmem][nlev][nij1] -> mean, spread [nv3d][nlev][nij1] and
+    [nv2d][nmem][nij1] -> [nv2d][nij1], in the state's dtype."""
+    lib = _abi.load()
+    s3, s2 = state3d.contiguous(), state2d.contiguous()
+    if s3.dtype not in (torch.float32, torch.float64) or s2.dtype != s3.dtype:
+        raise TypeError("state must be float32 or float64, both parts alike")
+    nv3d, k, nlev, nij1 = s3.shape
+    if (nv3d, k, nlev) != (params.nv3d, params.nmem, params.nlev) or tuple(s2.shape) != (params.nv2d, k, nij1):
+        raise ValueError("state shapes do not match the parameters")
+    m3 = torch.empty(nv3d, nlev, nij1, dtype=s3.dtype, device=s3.device)
+    d3 = torch.empty_like(m3)
+    m2 = torch.empty(params.nv2d, nij1, dtype=s2.dtype, device=s2.device)
+    d2 = torch.empty_like(m2)
+    cp = params.to_c()
+    _abi.check(lib.sbletkf_ensemble_mean_spread(ctypes.byref(cp), nij1, _ptr(s3), _ptr(s2),
+                                                F64 if s3.dtype == torch.float64 else F32, _ptr(m3), _ptr(d3),
+                                                _ptr(m2), _ptr(d2), _stream_ptr(stream)), "ensemble_mean_spread")
+    return m3, d3, m2, d2

@@ -211,4 +211,31 @@ int sbletkf_backward(sbletkf_workspace *ws, const sbletkf_params *p, const sblet
                          grad_rdiag, grad_infl, grad_sigma_obs, (cudaStream_t)stream);
 }
 
+int sbletkf_obs_operator(const sbletkf_params *p, const double *glon, const double *glat, const double *gfsm,
+                         const double *gdepth, const void *state3d, const void *state2d, int32_t state_dtype,
+                         const sbletkf_obs_in *obs, int32_t flags, const sbletkf_obs_out *out, double *stats,
+                         void *stream) {
+  int st = check_params(p);
+  if (st) return st;
+  if (!obs || !out || obs->nobs < 0) return SBLETKF_ERR_ARG;
+  if (p->nlev < 6) return SBLETKF_ERR_UNSUPPORTED;
+  if (state_dtype != SBLETKF_F32 && state_dtype != SBLETKF_F64) return SBLETKF_ERR_ARG;
+  if (obs->nobs > 0 && (!obs->elm || !obs->lon || !obs->lat || !obs->lev || !obs->dat || !obs->err || !glon ||
+                        !glat || !gfsm || !gdepth || (p->nv3d > 0 && !state3d) || (p->nv2d > 0 && !state2d)))
+    return SBLETKF_ERR_ARG;
+  return sbl::launch_obs_operator(p, glon, glat, gfsm, gdepth, state3d, state2d, state_dtype, obs, flags, out,
+                                  stats, (cudaStream_t)stream);
+}
+
+int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const void *state3d, const void *state2d,
+                                 int32_t state_dtype, void *mean3d, void *sprd3d, void *mean2d, void *sprd2d,
+                                 void *stream) {
+  if (!p || p->nmem < 1 || p->nmem > 128 || p->nlev < 1 || p->nv3d < 0 || p->nv2d < 0 || nij1 < 1)
+    return SBLETKF_ERR_ARG;
+  if (state_dtype != SBLETKF_F32 && state_dtype != SBLETKF_F64) return SBLETKF_ERR_ARG;
+  if ((p->nv3d > 0 && (!state3d || !mean3d)) || (p->nv2d > 0 && (!state2d || !mean2d))) return SBLETKF_ERR_ARG;
+  return sbl::launch_ens_mesp(p, nij1, state3d, state2d, state_dtype, mean3d, sprd3d, mean2d, sprd2d,
+                              (cudaStream_t)stream);
+}
+
 }  // extern "C"

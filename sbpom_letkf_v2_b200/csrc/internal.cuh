@@ -174,6 +174,11 @@ int launch_core_batched(const sbletkf_params *p, int32_t npts, const int64_t *of
                         const double *rdiag, const double *rloc, const double *dep, double *wvec,
                         double *wmat, const double *uni, int32_t *src, int32_t *pst, int *d_status,
                         cudaStream_t s);
+int launch_obs_operator(const sbletkf_params *p, const double *glon, const double *glat, const double *gfsm,
+                        const double *gdepth, const void *s3, const void *s2, int dtype, const sbletkf_obs_in *obs,
+                        int flags, const sbletkf_obs_out *out, double *stats, cudaStream_t s);
+int launch_ens_mesp(const sbletkf_params *p, int nij1, const void *s3, const void *s2, int dtype, void *m3, void *sd3,
+                    void *m2, void *sd2, cudaStream_t s);
 int launch_backward(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, const void *f3,
                     const void *f2, int dtype, const void *ga3, const void *ga2, double *gdep,
                     double *grdiag, double *ginfl, double *gsig, cudaStream_t s);

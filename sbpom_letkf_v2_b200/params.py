@@ -34,7 +34,8 @@ class CParams(ctypes.Structure):
         ("iswitch_da", ctypes.c_int32), ("nmonte", ctypes.c_int32), ("rm", ctypes.c_int32),
         ("dp", ctypes.c_int32), ("sr_textbook", ctypes.c_int32), ("roff", ctypes.c_int32),
         ("id_z_obs", ctypes.c_int32), ("precision", ctypes.c_int32),
-        ("max_sweeps", ctypes.c_int32), ("reserved_i", ctypes.c_int32 * 3),
+        ("max_sweeps", ctypes.c_int32),
+        ("iv3d_u", ctypes.c_int32), ("iv3d_v", ctypes.c_int32), ("iv2d_z", ctypes.c_int32),
         ("cov_infl_mul", ctypes.c_double), ("cov_infl_gm", ctypes.c_double),
         ("alpha_rtpp", ctypes.c_double), ("alpha_rtps", ctypes.c_double),
         ("sigma_obs", ctypes.c_double), ("sigma_obsv", ctypes.c_double),
@@ -71,6 +72,9 @@ class LETKFParams:
     id_z_obs: int = ID_Z_OBS        # :59
     precision: int = PREC_FP64
     max_sweeps: int = 40
+    iv3d_u: int = 0                 # :42 (1-based 1 -> 0-based 0)
+    iv3d_v: int = 1                 # :43
+    iv2d_z: int = 0                 # :46
     cov_infl_mul: float = 1.0       # :71
     cov_infl_gm: float = 1.0        # :89
     alpha_rtpp: float = 0.9         # :74
