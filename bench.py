@@ -203,6 +203,41 @@ def scaled_workload(wl, s: int):
                      name=wl.name + f" (1/{s} grid)")
 
 
+def aux_timings(case, p, dev) -> dict:
+    """The steps either side of the analysis on the same workload: the
+    observation operator (set_obs on the GPU) and the ensemble mean/spread of
+    the forecast; CUDA-event times, best of 3."""
+    from sbpom_letkf_v2_b200.analysis import ensemble_mean_spread
+    from sbpom_letkf_v2_b200.obsop import obs_operator
+    g = case.grid
+    grid = dict(lon=g["lon1"], lat=g["lat1"], fsm=(g["phi1"] != 1.0).double(), depth=g["depth1"])
+    o = case.obs
+    raw = dict(elm=o["elm"], lon=o["lon"], lat=o["lat"], lev=o["lev"], err=o["err"], dat=o["dep"])
+
+    def best(fn):
+        fn()
+        torch.cuda.synchronize()
+        t = 1e30
+        for _ in range(3):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            t = min(t, a.elapsed_time(b))
+        return t
+    nobs = int(o["elm"].numel())
+    t_op = best(lambda: obs_operator(p, grid, case.fcst3d, case.fcst2d, raw, stats=True))
+    t_ms = best(lambda: ensemble_mean_spread(p, case.fcst3d, case.fcst2d))
+    es = case.fcst3d.element_size()
+    by = (case.fcst3d.numel() + case.fcst2d.numel()) * es + 2 * (case.fcst3d.numel() + case.fcst2d.numel()) // p.nmem * es
+    peaks, _ = _peaks()
+    return {"obs_operator": {"ms": t_op, "obs_per_s": nobs / (t_op / 1e3), "nobs": nobs, "nmem": p.nmem},
+            "ensemble_mean_spread": {"ms": t_ms, "gbs": by / (t_ms / 1e3) / 1e9,
+                                     "frac_hbm": by / (t_ms / 1e3) / 1e9 / peaks["hbm_gbs"],
+                                     "bytes": by}}
+
+
 def config_of(wl, p, args, world) -> dict:
     """The workload description shared by both arms' JSON lines."""
     state_gb = 2.0 * 4.0 * wl.nmem * wl.nlon * wl.nlat * (4 * wl.nlev + 1) / 1e9
@@ -255,6 +290,8 @@ def main():
                     help="skip the one-step FP64-path measurement reported beside the mixed path")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying CUDA graphs")
+    ap.add_argument("--no-aux", action="store_true",
+                    help="skip the timing of the observation operator and the ensemble statistics")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--ref-seconds", type=float, default=8.0)
@@ -443,6 +480,9 @@ def main():
                 "mixed_error": mean_spread_error(m3, m2, a3, a2)}
         del m3, m2
 
+    aux = None
+    if not args.no_aux:
+        aux = aux_timings(case, p, dev)
     if rank == 0:
         fl = algorithmic_flops(nobsl, p.nmem, p.nv3d, p.nv2d, p.nlev, case.nij1)
         f64 = _fp64_peak(dev)
@@ -457,8 +497,12 @@ def main():
                     "note": "fused kernel: weights, nmonte draws and gather in one launch"}
         else:
             achieved = fl["total"] / (kern_ms / 1e3) / 1e12
+            # DRAM bytes per launch: ncu capture of the same kernel on the 1/8 grid
+            # (profiles/analysis_mixed_workload1_scale8_full.md), 220.2 MB for
+            # 74,000 points, scaled by the points of this launch
+            traffic = 220.2e6 / 74000.0 * P if (args.workload == 1 and prec == PREC_MIXED) else None
             roof = {"bound": "fp64", "achieved": achieved, "peak": f64["tflops"], "unit": "TFLOP/s",
-                    "frac": achieved / f64["tflops"], "traffic": None, "kernel": "k_analysis",
+                    "frac": achieved / f64["tflops"], "traffic": traffic, "kernel": "k_analysis",
                     "peak_source": f64["source"], "kernel_ms": kern_ms, "flops_per_launch": fl,
                     "note": "FP64 eigensolve bound"}
         cpu = None
@@ -472,6 +516,7 @@ def main():
                 "config": config_of(wl, p, args, world),
                 "nobsl": {"mean": float(nobsl.mean()), "max": int(nobsl.max()), "zero_frac": float((nobsl == 0).mean())},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "fp64_path": fp64,
+                "aux": aux,
                 "gpu_launches": 6 * args.steps, "graph": g_prep is not None, "peaks_source": src,
                 "hbm_peak_gbs": peaks.get("hbm_gbs")}
         print(json.dumps(line), flush=True)
