@@ -290,6 +290,8 @@ def main():
                     help="skip the one-step FP64-path measurement reported beside the mixed path")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying CUDA graphs")
+    ap.add_argument("--schedule", choices=["columns", "point"], default="columns",
+                    help="persistent column queue with warm-started eigensolves, or one CTA per point")
     ap.add_argument("--no-aux", action="store_true",
                     help="skip the timing of the observation operator and the ensemble statistics")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -331,6 +333,7 @@ def main():
     p = case.params.replace(precision=prec)
     nobs = case.obs["elm"].numel()
     an = Analysis(p, case.nij1, nobs, device=dev)
+    an.set_schedule(Analysis.SCHED_COLUMNS if args.schedule == "columns" else Analysis.SCHED_POINT)
     an.prepare_obs(case.obs)
     nobsl = an.count_nobsl(case.grid).cpu().numpy()
     a3 = torch.empty_like(case.fcst3d)
@@ -517,7 +520,7 @@ def main():
                 "nobsl": {"mean": float(nobsl.mean()), "max": int(nobsl.max()), "zero_frac": float((nobsl == 0).mean())},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "fp64_path": fp64,
                 "aux": aux,
-                "gpu_launches": 6 * args.steps, "graph": g_prep is not None, "peaks_source": src,
+                "gpu_launches": 6 * args.steps, "graph": g_prep is not None, "schedule": args.schedule, "peaks_source": src,
                 "hbm_peak_gbs": peaks.get("hbm_gbs")}
         print(json.dumps(line), flush=True)
     an.close()

@@ -252,6 +252,18 @@ int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const vo
                                  int32_t state_dtype, void *mean3d, void *sprd3d, void *mean2d, void *sprd2d,
                                  void *stream);
 
+/* Launch schedule of sbletkf_analysis for this workspace.
+ * SBLETKF_SCHED_COLUMNS (the default): one persistent CTA per SM takes grid
+ * columns from an atomic queue and analyses each column's levels from the
+ * surface down, starting every k x k eigensolve from the eigenvectors of the
+ * column's previous level.  SBLETKF_SCHED_POINT: one CTA per grid point,
+ * every eigensolve from scratch.  Both give the same analysis to rounding.
+ * No reference counterpart (the reference's OpenMP DYNAMIC loop over (k,i),
+ * common_da.f90:66-68, is the scheduling it replaces). */
+#define SBLETKF_SCHED_POINT   0
+#define SBLETKF_SCHED_COLUMNS 1
+int sbletkf_workspace_set_schedule(sbletkf_workspace *ws, int32_t schedule);
+
 /* Vector-Jacobian product of the LETKF analysis (iswitch_da = 1, with RTPP,
  * RTPS and the T/S round-off): given dJ/d anal3d and dJ/d anal2d (same layouts
  * as the state, state_dtype), accumulate dJ/d dep and dJ/d rdiag ([nobs],

@@ -62,6 +62,13 @@ class Analysis:
         self._keep = []
         self.nobs = None
 
+    SCHED_POINT, SCHED_COLUMNS = 0, 1
+
+    def set_schedule(self, schedule: int) -> None:
+        """SCHED_COLUMNS (default): persistent column queue with warm-started
+        eigensolves; SCHED_POINT: one CTA per grid point."""
+        _abi.check(self.lib.sbletkf_workspace_set_schedule(self._ws, int(schedule)), "set_schedule")
+
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
         if self._ws:

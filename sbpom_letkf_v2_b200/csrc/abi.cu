@@ -84,6 +84,14 @@ int sbletkf_workspace_create(const sbletkf_params *p, int32_t nij1, int32_t max_
   alloc((void **)&ws->d_cellcnt, sizeof(int32_t) * ws->ncell);
   alloc((void **)&ws->d_status, sizeof(int32_t) * 4);
   alloc((void **)&ws->d_gscratch, sizeof(double) * 8);
+  {  // persistent schedule: one CTA per SM, two k x k FP64 matrices each
+    int nsm = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    ws->nslab = nsm;
+    alloc((void **)&ws->d_queue, sizeof(int32_t) * 4);
+    alloc((void **)&ws->d_slab, sizeof(double) * 2 * (size_t)p->nmem * p->nmem * (size_t)(nsm > 0 ? nsm : 1));
+    ws->schedule = 1;
+  }
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ws->h_status, sizeof(int32_t) * 4);
   if (e == cudaSuccess) e = cudaMemset(ws->d_status, 0, sizeof(int32_t) * 4);
   if (e == cudaSuccess) e = cudaMemset(ws->d_cellstart, 0, sizeof(int32_t) * (ws->ncell + 1));
@@ -100,7 +108,7 @@ int sbletkf_workspace_destroy(sbletkf_workspace *ws) {
   cudaSetDevice(ws->device);
   void *ptrs[] = {ws->d_elm, ws->d_lon, ws->d_lat, ws->d_lev, ws->d_rdiag, ws->d_dep, ws->d_hdxf64,
                   ws->d_hdxf32, ws->d_perm, ws->d_tmp, ws->d_cellstart, ws->d_cellcnt, ws->d_status,
-                  ws->d_gscratch};
+                  ws->d_gscratch, ws->d_queue, ws->d_slab};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (ws->h_status) cudaFreeHost(ws->h_status);
@@ -152,6 +160,12 @@ int sbletkf_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const sblet
   }
   return launch_analysis(ws, p, grid_view(grid), fcst3d, fcst2d, anal3d, anal2d, state_dtype, uniforms,
                          resample_src, point_status, s);
+}
+
+int sbletkf_workspace_set_schedule(sbletkf_workspace *ws, int32_t schedule) {
+  if (!ws || (schedule != SBLETKF_SCHED_POINT && schedule != SBLETKF_SCHED_COLUMNS)) return SBLETKF_ERR_ARG;
+  ws->schedule = schedule;
+  return SBLETKF_OK;
 }
 
 int sbletkf_count_nobsl(sbletkf_workspace *ws, const sbletkf_params *p, const sbletkf_grid *grid, int32_t *nobsl,

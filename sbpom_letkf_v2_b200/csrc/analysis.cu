@@ -107,7 +107,7 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
   if (tid < kKC) sw[tid] = tid < cnt ? (float)sqrt(S.lw[f + tid]) : 0.0f;
   __syncthreads();
   st.broken = s_broken;
-  if (!st.broken && st.uses[s] > 0) {  // the chunk two back is complete: add it to the sum
+  if (!st.broken && st.nchunk >= 2) {  // this point's chunk two back is complete: add it to the sum
     fence_after_sync();
     tc_flush<KP>(st, s);
     fence_before_sync();
@@ -203,51 +203,42 @@ __device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint6
   __syncthreads();
 }
 
+// Analysis of grid point pid by the whole CTA (the body of the (k,i) loop of
+// da_main).  With vprev != nullptr (persistent, column-ordered launch) a
+// primal eigensolve starts from the eigenvectors of the previous level of
+// the same column when `warm` is set, and leaves its own there.
 template <int R, typename ST, bool MIXED>
-__global__ void __launch_bounds__(kThreads, 1)
-    k_analysis(const sbletkf_params p, const GridView g, const ObsView ob, const ST *__restrict__ f3,
-               const ST *__restrict__ f2, ST *__restrict__ a3, ST *__restrict__ a2, const double *__restrict__ uni,
-               int32_t *__restrict__ src_out, int32_t *__restrict__ pst, int *status, long long p0) {
+__device__ __forceinline__ void analyze_point(const sbletkf_params &p, const GridView &g, const ObsView &ob,
+                                              const ST *__restrict__ f3, const ST *__restrict__ f2,
+                                              ST *__restrict__ a3, ST *__restrict__ a2,
+                                              const double *__restrict__ uni, int32_t *__restrict__ src_out,
+                                              int32_t *__restrict__ pst, int *status, const PointSmem &S,
+                                              TcState &tcs, uint64_t *s_mbar, bool tc_on, long long pid,
+                                              double *vprev, double *xtmp, int &warm) {
   constexpr int KP = kp_of_r(R);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  PointSmem S;
   const int k = p.nmem;
-  S.carve(smem_raw, k, KP);
   const int tid = threadIdx.x;
-  const long long pid = p0 + blockIdx.x;
   const int nij1 = g.nij1, nlev = p.nlev;
   const int kl = (int)(pid / nij1), i = (int)(pid % nij1);
   const bool do_pf = p.iswitch_da != SBLETKF_DA_LETKF;
   const bool do_gram = p.iswitch_da != SBLETKF_DA_LPF;
   __shared__ int sh[8];
   __shared__ double shd[4];
-  __shared__ uint64_t s_mbar[2];
-  __shared__ uint32_t s_tmem;
   int bits = 0;
-  constexpr uint32_t kTmemCols = (4 * KP <= 128) ? 128 : (4 * KP <= 256) ? 256 : 512;
-  const bool tc_on = MIXED && do_gram;  // TMEM and barriers held by this CTA
-  TcState tcs;
-  tcs.uses[0] = tcs.uses[1] = 0;
-  tcs.nchunk = 0;
-  tcs.nflushed = 0;
-  tcs.tbase = 0;
-  tcs.broken = 0;
   if (tc_on) {
     // after a tensor-core wait has timed out anywhere in the launch, later
-    // CTAs return at once (the status word already carries the error)
+    // points return at once (the status word already carries the error)
     __shared__ int s_abort;
     if (tid == 0) s_abort = (*(volatile int *)status & SBLETKF_ERR_TIMEOUT) != 0;
     __syncthreads();
-    if (s_abort) {
+    const int ab = s_abort;
+    __syncthreads();
+    if (ab) {
       if (tid == 0 && pst) pst[pid] = SBLETKF_ERR_TIMEOUT;
       return;
     }
-    if ((tid >> 5) == 0) tc::tmem_alloc(&s_tmem, kTmemCols);
-    if (tid == 0) {
-      tc::mbar_init(&s_mbar[0], 1);
-      tc::mbar_init(&s_mbar[1], 1);
-    }
-    tc::fence_before_sync();
+    tcs.nchunk = 0;
+    tcs.nflushed = 0;
   }
 
   // ---- search box and its grid rows (common_da.f90:158-161, 314-346)
@@ -270,10 +261,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   __syncthreads();
   bits |= sh[5];
-  if (tc_on) {
-    tc::fence_after_sync();
-    tcs.tbase = s_tmem;
-  }
   const int imin = sh[0], imax = sh[1], jmin = sh[2], nrows = sh[4];
   const double rdep = shd[0], plon = shd[1], plat = shd[2], phi = shd[3];
   {
@@ -455,7 +442,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (use_tc) tc_finish<KP>(S, tcs, s_mbar, k, alpha, A.b, bits);
     else store_gram<R>(S, k, alpha, A);
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
-    bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+    if (vprev && warm)  // start from the previous level's eigenvectors
+      bits |= jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.cw, vprev, xtmp);
+    else
+      bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+    if (vprev) {  // keep this level's eigenvectors for the next one
+      for (int e = tid; e < k * k; e += kThreads) vprev[e] = S.u[(long)(e / k) * S.ldb + (e % k)];
+      warm = 1;
+    }
     vt_times(S.u, k, S.ldb, S.b, S.c);  // c = Lambda^-1 V^T b
     __syncthreads();
     if (tid < k) S.c[tid] /= S.lam[tid];
@@ -619,14 +613,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     else a2[((long)(v - p.nv3d) * k + m) * nij1 + i] = (ST)a;
   }
   if (tc_on && (bits & SBLETKF_ERR_TIMEOUT)) atomicOr(status, SBLETKF_ERR_TIMEOUT);
-  if (tc_on) {  // every UMMA was waited for in tc_finish (or never issued)
-    tc::fence_before_sync();
-    __syncthreads();
-    if ((tid >> 5) == 0) {
-      tc::fence_after_sync();
-      tc::tmem_dealloc(tcs.tbase, kTmemCols);
-    }
-  }
   __shared__ int s_bits;
   if (tid == 0) s_bits = 0;
   __syncthreads();
@@ -636,6 +622,90 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (tid == 0) {
     if (pst) pst[pid] = bits;
     if (bits) atomicOr(status, bits);
+  }
+}
+
+// One CTA per grid point (queue == nullptr; point p0 + blockIdx.x), or a
+// persistent launch of one CTA per SM taking grid columns from the atomic
+// counter *queue and analysing each column's levels from the surface down,
+// warm-starting every primal eigensolve from the previous level
+// (slab: 2 k x k FP64 scratch matrices per CTA).
+template <int R, typename ST, bool MIXED>
+__global__ void __launch_bounds__(kThreads, 1)
+    k_analysis(const sbletkf_params p, const GridView g, const ObsView ob, const ST *__restrict__ f3,
+               const ST *__restrict__ f2, ST *__restrict__ a3, ST *__restrict__ a2, const double *__restrict__ uni,
+               int32_t *__restrict__ src_out, int32_t *__restrict__ pst, int *status, long long p0, int *queue,
+               double *slab) {
+  constexpr int KP = kp_of_r(R);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PointSmem S;
+  const int k = p.nmem;
+  S.carve(smem_raw, k, KP);
+  const int tid = threadIdx.x;
+  const bool do_gram = p.iswitch_da != SBLETKF_DA_LPF;
+  __shared__ uint64_t s_mbar[2];
+  __shared__ uint32_t s_tmem;
+  constexpr uint32_t kTmemCols = (4 * KP <= 128) ? 128 : (4 * KP <= 256) ? 256 : 512;
+  const bool tc_on = MIXED && do_gram;  // TMEM and barriers held by this CTA
+  TcState tcs;
+  tcs.uses[0] = tcs.uses[1] = 0;
+  tcs.nchunk = 0;
+  tcs.nflushed = 0;
+  tcs.tbase = 0;
+  tcs.broken = 0;
+  if (tc_on) {
+    __shared__ int s_abort;
+    if (tid == 0) s_abort = (*(volatile int *)status & SBLETKF_ERR_TIMEOUT) != 0;
+    __syncthreads();
+    if (s_abort) {
+      if (tid == 0 && pst && !queue) pst[p0 + blockIdx.x] = SBLETKF_ERR_TIMEOUT;
+      return;
+    }
+    if ((tid >> 5) == 0) tc::tmem_alloc(&s_tmem, kTmemCols);
+    if (tid == 0) {
+      tc::mbar_init(&s_mbar[0], 1);
+      tc::mbar_init(&s_mbar[1], 1);
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    tcs.tbase = s_tmem;
+  }
+  // one call site of the point body for both schedules
+  double *vprev = queue ? slab + (size_t)blockIdx.x * 2 * k * k : nullptr;
+  double *xtmp = queue ? vprev + (size_t)k * k : nullptr;
+  __shared__ int s_item;
+  int warm = 0, col = 0, kl = -1;
+  bool first = true;
+  for (;;) {
+    long long pid;
+    if (queue) {
+      if (kl < 0) {  // next column from the queue, levels from the surface down
+        if (tid == 0) s_item = atomicAdd(queue, 1);
+        __syncthreads();
+        col = s_item;
+        __syncthreads();
+        if (col >= g.nij1) break;
+        kl = p.nlev - 1;
+        warm = 0;
+      }
+      pid = (long long)kl * g.nij1 + col;
+      --kl;
+    } else {
+      if (!first) break;
+      first = false;
+      pid = p0 + blockIdx.x;
+    }
+    analyze_point<R, ST, MIXED>(p, g, ob, f3, f2, a3, a2, uni, src_out, pst, status, S, tcs, s_mbar, tc_on, pid,
+                                vprev, xtmp, warm);
+  }
+  if (tc_on) {  // every UMMA was waited for in tc_finish (or never issued)
+    tc::fence_before_sync();
+    __syncthreads();
+    if ((tid >> 5) == 0) {
+      tc::fence_after_sync();
+      tc::tmem_dealloc(tcs.tbase, kTmemCols);
+    }
   }
 }
 
@@ -667,36 +737,49 @@ __global__ void k_count(const sbletkf_params p, const GridView g, const ObsView 
   (void)status;
 }
 
+struct Sched {
+  int *queue;    // nullptr: one CTA per point
+  double *slab;
+  int ctas;
+};
+
 template <int R, typename ST, bool MIXED>
 int launch_r(const sbletkf_params *p, const GridView &g, const ObsView &ob, const void *f3, const void *f2, void *a3,
-             void *a2, const double *uni, int32_t *src, int32_t *pst, int *status, cudaStream_t s) {
+             void *a2, const double *uni, int32_t *src, int32_t *pst, int *status, const Sched &sc, cudaStream_t s) {
   const size_t smem = PointSmem::bytes(p->nmem, kp_of_r(R), MIXED);
   auto kern = k_analysis<R, ST, MIXED>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_status(e);
+  if (sc.queue) {
+    e = cudaMemsetAsync(sc.queue, 0, sizeof(int), s);
+    if (e != cudaSuccess) return cuda_status(e);
+    kern<<<(unsigned)sc.ctas, kThreads, smem, s>>>(*p, g, ob, (const ST *)f3, (const ST *)f2, (ST *)a3, (ST *)a2,
+                                                    uni, src, pst, status, 0, sc.queue, sc.slab);
+    return cuda_status(cudaGetLastError());
+  }
   const long long P = (long long)p->nlev * g.nij1;
   const long long maxg = 2147483647LL;
   for (long long p0 = 0; p0 < P; p0 += maxg) {
     const long long n = P - p0 < maxg ? P - p0 : maxg;
     kern<<<(unsigned)n, kThreads, smem, s>>>(*p, g, ob, (const ST *)f3, (const ST *)f2, (ST *)a3, (ST *)a2, uni,
-                                              src, pst, status, p0);
+                                              src, pst, status, p0, nullptr, nullptr);
   }
   return cuda_status(cudaGetLastError());
 }
 
 template <typename ST>
 int launch_t(const sbletkf_params *p, const GridView &g, const ObsView &ob, const void *f3, const void *f2, void *a3,
-             void *a2, const double *uni, int32_t *src, int32_t *pst, int *status, cudaStream_t s) {
+             void *a2, const double *uni, int32_t *src, int32_t *pst, int *status, const Sched &sc, cudaStream_t s) {
   const bool mixed = p->precision == SBLETKF_PREC_MIXED;
   switch (r_for_k(p->nmem)) {
-    case 2: return mixed ? launch_r<2, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s)
-                         : launch_r<2, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
-    case 4: return mixed ? launch_r<4, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s)
-                         : launch_r<4, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
-    case 7: return mixed ? launch_r<7, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s)
-                         : launch_r<7, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
-    default: return mixed ? launch_r<8, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s)
-                          : launch_r<8, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, s);
+    case 2: return mixed ? launch_r<2, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, sc, s)
+                         : launch_r<2, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, sc, s);
+    case 4: return mixed ? launch_r<4, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, sc, s)
+                         : launch_r<4, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, sc, s);
+    case 7: return mixed ? launch_r<7, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, sc, s)
+                         : launch_r<7, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, sc, s);
+    default: return mixed ? launch_r<8, ST, true>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, sc, s)
+                          : launch_r<8, ST, false>(p, g, ob, f3, f2, a3, a2, uni, src, pst, status, sc, s);
   }
 }
 
@@ -706,8 +789,10 @@ int launch_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const GridVi
                     const void *f2, void *a3, void *a2, int dtype, const double *uni, int32_t *src, int32_t *pst,
                     cudaStream_t s) {
   const ObsView ob = ws->obs_view();
-  if (dtype == SBLETKF_F64) return launch_t<double>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, s);
-  return launch_t<float>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, s);
+  Sched sc{nullptr, nullptr, 0};
+  if (ws->schedule == 1 && ws->d_queue && ws->d_slab) sc = Sched{ws->d_queue, ws->d_slab, ws->nslab};
+  if (dtype == SBLETKF_F64) return launch_t<double>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, sc, s);
+  return launch_t<float>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, sc, s);
 }
 
 int launch_count(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, int32_t *nobsl,

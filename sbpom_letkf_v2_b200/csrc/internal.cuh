@@ -149,6 +149,12 @@ struct sbletkf_workspace {
   int32_t *d_status;
   int32_t *h_status;  // pinned
   double *d_gscratch; // backward scalar accumulators [2]
+  // analysis schedule: 0 = one CTA per point, 1 = persistent column queue
+  // with warm-started eigensolves (d_queue counter, d_slab 2 k x k FP64 per CTA)
+  int schedule = 0;
+  int nslab = 0;
+  int32_t *d_queue = nullptr;
+  double *d_slab = nullptr;
   sbl::ObsView obs_view() const {
     sbl::ObsView v;
     v.nobs = nobs; v.ldh = ldh; v.elm = d_elm; v.lon = d_lon; v.lat = d_lat; v.lev = d_lev;

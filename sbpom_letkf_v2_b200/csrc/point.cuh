@@ -405,6 +405,71 @@ static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, doub
   return bits;
 }
 
+// Eigenpairs of the SPD matrix in B from a starting orthogonal matrix V
+// (n x n in global memory, column j at V + j*n; the eigenvectors of a nearby
+// matrix): one-sided Jacobi on the columns of X = A V (X in global scratch,
+// then in B).  Since X X^T = A^2, the converged columns are lambda_j u_j:
+// lambda_j = |column j|, u_j = column / lambda_j.  When A is close to the
+// matrix V came from, X starts nearly orthogonal and needs a few sweeps
+// instead of the cold solve's pivoted Cholesky and ~10 sweeps.
+template <int EMAX>
+static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb, double tol, int maxsw, double *lam,
+                                                      int *flag, double *vec, const double *V, double *X) {
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+  // X = A V, 4 columns of V per thread pass (A symmetric, column q of A = row q)
+  for (int e = tid; e < n * ((n + 3) / 4); e += nt) {
+    const int r = e % n, c0 = (e / n) * 4;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    const double *v0 = V + (long)c0 * n;
+    for (int q = 0; q < n; ++q) {
+      const double a = B[(long)q * ldb + r];
+      s0 = fma(a, v0[q], s0);
+      if (c0 + 1 < n) s1 = fma(a, v0[n + q], s1);
+      if (c0 + 2 < n) s2 = fma(a, v0[2 * n + q], s2);
+      if (c0 + 3 < n) s3 = fma(a, v0[3 * n + q], s3);
+    }
+    X[(long)c0 * n + r] = s0;
+    if (c0 + 1 < n) X[(long)(c0 + 1) * n + r] = s1;
+    if (c0 + 2 < n) X[(long)(c0 + 2) * n + r] = s2;
+    if (c0 + 3 < n) X[(long)(c0 + 3) * n + r] = s3;
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += nt) B[(long)(e / n) * ldb + (e % n)] = X[e];
+  __syncthreads();
+  int bits = 0;
+  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps<8>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, maxsw, vec, flag);
+  else bits |= jacobi_sweeps<EMAX>(B, n, ldb, tol, maxsw, vec, flag);
+  for (int j = wid; j < n; j += nw) {
+    double *cj = B + (long)j * ldb;
+    double v[4], s = 0.0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int r = lane + 32 * t;
+      v[t] = r < n ? cj[r] : 0.0;
+      s = fma(v[t], v[t], s);
+    }
+    s = __shfl_sync(0xffffffffu, warp_sum(s), 0);
+    const double l = sqrt(s);
+    if (lane == 0) lam[j] = l;
+    const double inv = 1.0 / l;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int r = lane + 32 * t;
+      if (r < n) cj[r] = v[t] * inv;
+    }
+  }
+  if (threadIdx.x == 0) flag[1] = 0;
+  __syncthreads();
+  for (int j = threadIdx.x; j < n; j += blockDim.x)
+    if (!(lam[j] > 0.0) || !isfinite(lam[j])) atomicOr(flag + 1, SBLETKF_ERR_NONFINITE);
+  __syncthreads();
+  bits |= flag[1];
+  return bits;
+}
+
 // out[v*ldo + j] = sum_m X[v*ldx + m] V[m][j] for v < nv, j < n: warp per
 // column j, lanes over rows m (contiguous in a column of V).
 static __device__ __forceinline__ void x_times_v(const double *X, int ldx, int nv, const double *V, int n, int ldb,

@@ -17,10 +17,12 @@ pytestmark = pytest.mark.gpu
 TOL64 = 1e-10
 
 
-def run_gpu(p, grid, obs, f3, f2, uni=None, dtype=torch.float64, want_src=False, dev="cuda:0"):
+def run_gpu(p, grid, obs, f3, f2, uni=None, dtype=torch.float64, want_src=False, dev="cuda:0", schedule=None):
     t = lambda a, dt=None: torch.as_tensor(np.asarray(a), device=dev, dtype=dt)
     nij1 = grid["lon1"].size
     an = Analysis(p, nij1, max(1, obs["elm"].size), device=dev)
+    if schedule is not None:
+        an.set_schedule(schedule)
     an.prepare_obs({k: t(v) for k, v in obs.items()})
     g = {k: t(v, torch.float64) for k, v in grid.items()}
     src = None
@@ -191,3 +193,22 @@ def test_mixed_dense_points_route_to_fp64_gram(cuda):
     assert r["nobsl"].max() > 12288   # every search box here holds 14,040 candidates
     em, es = _mean_spread_err(r["anal3d"], ref["anal3d"])
     assert em <= TOL_MIXED and es <= TOL_MIXED
+
+
+@pytest.mark.parametrize("k,precision", [(20, 0), (64, 0), (100, 0), (100, 1)])
+def test_both_schedules_match_the_oracle(k, precision, cuda):
+    """One CTA per point (every eigensolve cold) and the persistent column
+    queue (eigensolves warm-started from the level above) agree with the
+    oracle and with each other."""
+    case = _case(k, cov_infl_mul=1.1, alpha_rtps=0.4)
+    g, ob, f3, f2 = _np(case)
+    ref = cref.da_main(case.params, g, ob, f3, f2, rsize=8)
+    p = case.params.replace(precision=precision)
+    r0 = run_gpu(p, g, ob, f3, f2, schedule=Analysis.SCHED_POINT)
+    r1 = run_gpu(p, g, ob, f3, f2, schedule=Analysis.SCHED_COLUMNS)
+    tol = TOL64 if precision == 0 else TOL_MIXED
+    for r in (r0, r1):
+        assert (r["status"] == 0).all()
+        assert field_relerr(r["anal3d"], ref["anal3d"]) <= tol
+        assert field_relerr(r["anal2d"], ref["anal2d"]) <= tol
+    assert field_relerr(r1["anal3d"], r0["anal3d"]) <= (1e-12 if precision == 0 else 1e-6)
