@@ -1,4 +1,4 @@
-// analysis.cu -- the analysis step, one CTA per grid point (FP64 path).
+// analysis.cu -- the analysis step: a CTA analyses one grid point at a time.
 //
 // Replaces the body of the (k,i) loop of da_main (letkf/run/src/common_da.f90:
 // 67-116): local observation selection (count_nobsl / obs_local, :133-293) as a
