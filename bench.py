@@ -290,6 +290,8 @@ def main():
                     help="skip the one-step FP64-path measurement reported beside the mixed path")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying CUDA graphs")
+    ap.add_argument("--tune", action="store_true",
+                    help="pick schedule and tensor-core routing with the autotuner before timing")
     ap.add_argument("--schedule", choices=["columns", "point"], default="columns",
                     help="persistent column queue with warm-started eigensolves, or one CTA per point")
     ap.add_argument("--no-aux", action="store_true",
@@ -334,6 +336,15 @@ def main():
     nobs = case.obs["elm"].numel()
     an = Analysis(p, case.nij1, nobs, device=dev)
     an.set_schedule(Analysis.SCHED_COLUMNS if args.schedule == "columns" else Analysis.SCHED_POINT)
+    tuned = None
+    if args.tune:
+        from sbpom_letkf_v2_b200 import tune
+        uni0 = (pf_uniforms(wl.npoints, p.nmonte, p.nmem, p.rm, device=dev, seed=11 + rank)
+                if p.iswitch_da != 1 else None)
+        tuned = tune.tune(p, case.grid, case.fcst3d, case.fcst2d, case.obs, uniforms=uni0, cache=None)
+        p = tune.apply(an, p, tuned)
+        an.params = p
+        an._cp = p.to_c()
     an.prepare_obs(case.obs)
     nobsl = an.count_nobsl(case.grid).cpu().numpy()
     a3 = torch.empty_like(case.fcst3d)
@@ -520,7 +531,7 @@ def main():
                 "nobsl": {"mean": float(nobsl.mean()), "max": int(nobsl.max()), "zero_frac": float((nobsl == 0).mean())},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(), "fp64_path": fp64,
                 "aux": aux,
-                "gpu_launches": 6 * args.steps, "graph": g_prep is not None, "schedule": args.schedule, "peaks_source": src,
+                "gpu_launches": 6 * args.steps, "graph": g_prep is not None, "schedule": args.schedule if tuned is None else tuned, "peaks_source": src,
                 "hbm_peak_gbs": peaks.get("hbm_gbs")}
         print(json.dumps(line), flush=True)
     an.close()

@@ -101,7 +101,9 @@ typedef struct sbletkf_params {
   double re;           /* earth radius [m]           (:28)                    */
   double pi;           /* (:27)                                               */
   double jacobi_tol;   /* relative off-diagonal tolerance of the eigensolve   */
-  double reserved_d[3];
+  double tc_max_cand;  /* mixed path: points whose search box holds more candidates
+                          use the FP64 Gram; <= 0: library default 12288   */
+  double reserved_d[2];
 } sbletkf_params;
 
 /* Local grid of the points analysed (set_common_mpi_pom, common_pom.f90:125-219) */

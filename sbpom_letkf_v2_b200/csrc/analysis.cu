@@ -294,7 +294,7 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
   const int ncand = S.rowpref[nrows];
   // FP32 accumulation in tensor memory is accurate to ~eps32 sqrt(n/16) |G|;
   // points whose search box holds more candidates take the FP64 Gram
-  const bool use_tc = tc_on && ncand <= tc::kMaxCand;
+  const bool use_tc = tc_on && (double)ncand <= (p.tc_max_cand > 0.0 ? p.tc_max_cand : (double)tc::kMaxCand);
 
   // ---- streaming local-obs selection + accumulation (obs order preserved).
   // Rows are consumed on the fly once nobsl exceeds the dual limit; below it

@@ -43,7 +43,8 @@ class CParams(ctypes.Structure):
         ("tmin", ctypes.c_double), ("tmax", ctypes.c_double),
         ("smin", ctypes.c_double), ("smax", ctypes.c_double),
         ("re", ctypes.c_double), ("pi", ctypes.c_double),
-        ("jacobi_tol", ctypes.c_double), ("reserved_d", ctypes.c_double * 3),
+        ("jacobi_tol", ctypes.c_double), ("tc_max_cand", ctypes.c_double),
+        ("reserved_d", ctypes.c_double * 2),
     ]
 
 
@@ -90,6 +91,7 @@ class LETKFParams:
     re: float = 6371.3e3            # :28
     pi: float = 4.0 * math.atan(1.0)  # :27
     jacobi_tol: float = 0.0         # 0 -> library default (k * eps)
+    tc_max_cand: float = 0.0        # mixed path: FP64 Gram above this many box candidates (0 -> 12288)
 
     def __post_init__(self):
         if self.dist_zero is None:
