@@ -512,9 +512,10 @@ def main():
         else:
             achieved = fl["total"] / (kern_ms / 1e3) / 1e12
             # DRAM bytes per launch: ncu capture of the same kernel on the 1/8 grid
-            # (profiles/analysis_mixed_workload1_scale8_full.md), 220.2 MB for
+            # (profiles/analysis_mixed_workload1_scale8_full.md), 274.7 MB for
             # 74,000 points, scaled by the points of this launch
-            traffic = 220.2e6 / 74000.0 * P if (args.workload == 1 and prec == PREC_MIXED) else None
+            traffic = (274.7e6 / 74000.0 * P if (args.workload == 1 and prec == PREC_MIXED
+                                                 and args.schedule == "columns") else None)
             roof = {"bound": "fp64", "achieved": achieved, "peak": f64["tflops"], "unit": "TFLOP/s",
                     "frac": achieved / f64["tflops"], "traffic": traffic, "kernel": "k_analysis",
                     "peak_source": f64["source"], "kernel_ms": kern_ms, "flops_per_launch": fl,
