@@ -626,9 +626,9 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
 }
 
 // One CTA per grid point (queue == nullptr; point p0 + blockIdx.x), or a
-// persistent launch of one CTA per SM taking grid columns from the atomic
-// counter *queue and analysing each column's levels from the surface down,
-// warm-starting every primal eigensolve from the previous level
+// persistent launch of one CTA per SM taking chunks of adjacent grid columns
+// from the atomic counter *queue and analysing their levels in snake order,
+// warm-starting every primal eigensolve from the previous primal point
 // (slab: 2 k x k FP64 scratch matrices per CTA).
 template <int R, typename ST, bool MIXED>
 __global__ void __launch_bounds__(kThreads, 1)
@@ -671,26 +671,40 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc::fence_after_sync();
     tcs.tbase = s_tmem;
   }
-  // one call site of the point body for both schedules
+  // one call site of the point body for both schedules.  Column schedule: a
+  // queue item is kColChunk adjacent columns, walked in snake order (levels
+  // down, then up, ...), so every column's first level with a primal
+  // eigensolve starts from the same level of the column beside it and every
+  // later level from the level above or below.
+  constexpr int kColChunk = 8;
   double *vprev = queue ? slab + (size_t)blockIdx.x * 2 * k * k : nullptr;
   double *xtmp = queue ? vprev + (size_t)k * k : nullptr;
   __shared__ int s_item;
-  int warm = 0, col = 0, kl = -1;
+  int warm = 0, col = 0, cend = 0, kl = 0, step = 1, remaining = 0;
   bool first = true;
   for (;;) {
     long long pid;
     if (queue) {
-      if (kl < 0) {  // next column from the queue, levels from the surface down
-        if (tid == 0) s_item = atomicAdd(queue, 1);
-        __syncthreads();
-        col = s_item;
-        __syncthreads();
-        if (col >= g.nij1) break;
-        kl = p.nlev - 1;
-        warm = 0;
+      if (remaining == 0) {  // next column
+        ++col;
+        if (col >= cend) {   // next chunk of columns from the queue
+          if (tid == 0) s_item = atomicAdd(queue, 1);
+          __syncthreads();
+          const long long c0 = (long long)s_item * kColChunk;
+          __syncthreads();
+          if (c0 >= g.nij1) break;
+          col = (int)c0;
+          cend = (int)(c0 + kColChunk < g.nij1 ? c0 + kColChunk : g.nij1);
+          warm = 0;
+          step = 1;
+        }
+        step = -step;        // surface-down first, then bottom-up, ...
+        kl = step < 0 ? p.nlev - 1 : 0;
+        remaining = p.nlev;
       }
       pid = (long long)kl * g.nij1 + col;
-      --kl;
+      kl += step;
+      --remaining;
     } else {
       if (!first) break;
       first = false;
