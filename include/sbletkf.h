@@ -255,11 +255,11 @@ int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const vo
                                  void *stream);
 
 /* Launch schedule of sbletkf_analysis for this workspace.
- * SBLETKF_SCHED_COLUMNS (the default): one persistent CTA per SM takes grid
- * columns from an atomic queue and analyses each column's levels from the
- * surface down, starting every k x k eigensolve from the eigenvectors of the
- * column's previous level.  SBLETKF_SCHED_POINT: one CTA per grid point,
- * every eigensolve from scratch.  Both give the same analysis to rounding.
+ * SBLETKF_SCHED_COLUMNS (the default, except for the LPF): one persistent CTA
+ * per SM takes chunks of adjacent grid columns from an atomic queue and walks
+ * their levels in snake order, starting every k x k eigensolve from the
+ * eigenvectors of the previous one.  SBLETKF_SCHED_POINT (the LPF default,
+ * which has no eigensolve): one CTA per grid point.  Both give the same analysis to rounding.
  * No reference counterpart (the reference's OpenMP DYNAMIC loop over (k,i),
  * common_da.f90:66-68, is the scheduling it replaces). */
 #define SBLETKF_SCHED_POINT   0

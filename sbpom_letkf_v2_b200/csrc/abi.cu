@@ -90,7 +90,8 @@ int sbletkf_workspace_create(const sbletkf_params *p, int32_t nij1, int32_t max_
     ws->nslab = nsm;
     alloc((void **)&ws->d_queue, sizeof(int32_t) * 4);
     alloc((void **)&ws->d_slab, sizeof(double) * 2 * (size_t)p->nmem * p->nmem * (size_t)(nsm > 0 ? nsm : 1));
-    ws->schedule = 1;
+    // the LPF has no eigensolve to warm-start: one CTA per point suits it
+    ws->schedule = p->iswitch_da == SBLETKF_DA_LPF ? 0 : 1;
   }
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ws->h_status, sizeof(int32_t) * 4);
   if (e == cudaSuccess) e = cudaMemset(ws->d_status, 0, sizeof(int32_t) * 4);

@@ -139,17 +139,29 @@ __device__ __forceinline__ void accumulate_chunk(const PointSmem &S, int f, int 
       if (tid < KP) A.b = fma(S.lwd[f + cc], yr[tid], A.b);
     }
   }
-  if (do_pf && tid < k) {
+  if (do_pf) {
     // log_like(j) = log_like(j) - 0.5*(dep-hdxf)*(dep-hdxf)*rloc/rdiag, serial in
-    // obs order, no contraction (common_lpfgm.f90:64-69)
-    double ll = A.ll;
-    for (int cc = 0; cc < cnt; ++cc) {
-      double d = __dsub_rn(S.ldep[f + cc], S.u[cc * KP + tid]);
-      double q = __dmul_rn(__dmul_rn(0.5, d), d);
-      q = __ddiv_rn(__dmul_rn(q, S.lrloc[f + cc]), S.lrdiag[f + cc]);
-      ll = __dsub_rn(ll, q);
+    // obs order, no contraction (common_lpfgm.f90:64-69).  The terms are
+    // independent: the whole CTA computes them (in place of the rows, which the
+    // Gram above has finished with), then each member's thread subtracts its
+    // column of terms in observation order -- the same operations and order.
+    if (do_gram) __syncthreads();
+    double *q = S.u;
+#pragma unroll 4
+    for (int e = tid; e < cnt * KP; e += kThreads) {
+      const int cc = e / KP, m = e - cc * KP;
+      if (m < k) {
+        const double d = __dsub_rn(S.ldep[f + cc], q[e]);
+        double t = __dmul_rn(__dmul_rn(0.5, d), d);
+        q[e] = __ddiv_rn(__dmul_rn(t, S.lrloc[f + cc]), S.lrdiag[f + cc]);
+      }
     }
-    A.ll = ll;
+    __syncthreads();
+    if (tid < k) {
+      double ll = A.ll;
+      for (int cc = 0; cc < cnt; ++cc) ll = __dsub_rn(ll, q[cc * KP + tid]);
+      A.ll = ll;
+    }
   }
   __syncthreads();
 }
