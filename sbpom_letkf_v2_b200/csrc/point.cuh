@@ -375,6 +375,174 @@ static __device__ __forceinline__ int jacobi_sweeps(double *B, int n, int ldb, d
   return sweep >= maxsw ? SBLETKF_ERR_EIG_NOCONV : 0;
 }
 
+// The same one-sided sweeps with the odd-even ordering, columns held in
+// registers: 4-lane group g holds the columns at positions (2g, 2g+1) in odd
+// steps and (2g+1, 2g+2) in even steps (E rows per lane each).  After a
+// rotation the pair's columns trade positions, so after an odd step a group
+// passes one column (and its squared norm) to its left neighbour and after an
+// even step one to its right.  The columns travel through slots in B (the
+// matrix is in registers meanwhile): left-going slot g = column g of B,
+// right-going slot g = column ng+g, norms in nrm[] likewise; position 0 in
+// even steps stays parked in left slot 0.  Over n2 steps every pair of
+// columns meets once, as in a round-robin sweep, but each step moves one
+// column per pair through shared memory instead of loading and storing both,
+// with one barrier.  On exit B holds the columns in some order (the zero
+// padding column of odd n is dropped), which is all the eigenpair extraction
+// needs.  nrm: >= n doubles of scratch; flag: >= 4 shared ints.
+template <int E>
+static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb, double tol, int maxsw, double *nrm,
+                                                       int *flag) {
+  constexpr int G = 4;
+  const int tid = threadIdx.x, gl = tid % G, grp = tid / G, lane = tid & 31;
+  const int n2 = (n + 1) & ~1, ng = n2 / 2;   // 2*ng - 1 <= n slots fit in B
+  const bool inb = grp < ng;
+  double *SL = B, *SR = B + (long)ng * ldb, *NL = nrm, *NR = nrm + ng;
+  double x[E], y[E], nx = 0.0, ny = 0.0;
+  {  // load positions (2g, 2g+1) = columns 2g, 2g+1 (position n of odd n: zeros)
+    const int ca = 2 * grp, cb = 2 * grp + 1;
+#pragma unroll
+    for (int t = 0; t < E; ++t) {
+      const int r = gl + G * t;
+      x[t] = (inb && ca < n && r < n) ? B[(long)ca * ldb + r] : 0.0;
+      y[t] = (inb && cb < n && r < n) ? B[(long)cb * ldb + r] : 0.0;
+    }
+  }
+  __syncthreads();
+  const double tol2 = tol * tol, big2 = 1e-20;
+  int sweep = 0;
+  for (; sweep < maxsw; ++sweep) {
+    {  // exact squared norms at the start of a sweep
+      double a = 0.0, b = 0.0;
+#pragma unroll
+      for (int t = 0; t < E; ++t) {
+        a = fma(x[t], x[t], a);
+        b = fma(y[t], y[t], b);
+      }
+#pragma unroll
+      for (int o = G / 2; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+      }
+      nx = __shfl_sync(0xffffffffu, a, lane & ~(G - 1));
+      ny = __shfl_sync(0xffffffffu, b, lane & ~(G - 1));
+    }
+    if (tid == 0) *flag = 0;
+    __syncthreads();
+    int big = 0;
+    for (int step = 0; step < n2; ++step) {
+      const bool odd = (step & 1) == 0;
+      const bool act = inb && (odd || grp < ng - 1);
+      double g0 = 0.0, g1 = 0.0;
+#pragma unroll
+      for (int t = 0; t < E; ++t) {
+        if (t & 1) g1 = fma(x[t], y[t], g1);
+        else g0 = fma(x[t], y[t], g0);
+      }
+      double ga = g0 + g1;
+#pragma unroll
+      for (int o = G / 2; o > 0; o >>= 1) ga += __shfl_xor_sync(0xffffffffu, ga, o);
+      ga = __shfl_sync(0xffffffffu, ga, lane & ~(G - 1));
+      const double g2 = ga * ga, ab = nx * ny;
+      if (act && g2 > tol2 * ab) {
+        const float zf = __fdividef((float)(ny - nx) * 0.5f, (float)ga);
+        const float tf = copysignf(1.0f, zf) / (fabsf(zf) + sqrtf(fmaf(zf, zf, 1.0f)));
+        const double tt = (double)tf;
+        const double cs = rsqrt(fma(tt, tt, 1.0)), sn = cs * tt;
+#pragma unroll
+        for (int t = 0; t < E; ++t) {
+          const double a = x[t], b = y[t];
+          x[t] = cs * a - sn * b;
+          y[t] = sn * a + cs * b;
+        }
+        const double c2 = cs * cs, s2 = sn * sn, csg = 2.0 * cs * sn * ga;
+        const double nx2 = c2 * nx - csg + s2 * ny;
+        ny = s2 * nx + csg + c2 * ny;
+        nx = nx2;
+        if (g2 > big2 * ab) big = 1;
+      }
+      // the pair's columns trade positions: x is now at the second, y at the first
+      if (odd) {  // y to the left neighbour (group 0's stays parked), new y from the right
+        if (inb) {
+#pragma unroll
+          for (int t = 0; t < E; ++t) {
+            const int r = gl + G * t;
+            if (r < n) SL[(long)grp * ldb + r] = y[t];
+          }
+          if (gl == 0) NL[grp] = ny;
+        }
+        __syncthreads();
+        if (inb && grp + 1 < ng) {
+#pragma unroll
+          for (int t = 0; t < E; ++t) {
+            const int r = gl + G * t;
+            y[t] = r < n ? SL[(long)(grp + 1) * ldb + r] : 0.0;
+          }
+          ny = NL[grp + 1];
+        }
+      } else {    // x to the right neighbour, new x from the left (group 0: the parked column)
+        if (inb && grp == ng - 1) {  // idle last pair: its single column moves to y
+#pragma unroll
+          for (int t = 0; t < E; ++t) y[t] = x[t];
+          ny = nx;
+        }
+        if (inb && grp < ng - 1) {
+#pragma unroll
+          for (int t = 0; t < E; ++t) {
+            const int r = gl + G * t;
+            if (r < n) SR[(long)grp * ldb + r] = x[t];
+          }
+          if (gl == 0) NR[grp] = nx;
+        }
+        __syncthreads();
+        if (inb) {
+          const double *src = grp > 0 ? SR + (long)(grp - 1) * ldb : SL;
+#pragma unroll
+          for (int t = 0; t < E; ++t) {
+            const int r = gl + G * t;
+            x[t] = r < n ? src[r] : 0.0;
+          }
+          nx = grp > 0 ? NR[grp - 1] : NL[0];
+        }
+      }
+      // no second barrier: the next step writes the other slot area, and a
+      // slot is rewritten only after the following step's barrier
+    }
+    if (big) *flag = 1;
+    __syncthreads();
+    const int rot = *flag;
+    __syncthreads();
+    if (!rot) break;
+  }
+  if (tid == 0) flag[3] = sweep;  // sweeps run (diagnostics)
+  // write the columns back; for odd n one position holds the zero padding
+  // column (squared norm exactly 0: it never rotates), whose place takes the
+  // column at position n
+  if (tid == 0) flag[2] = -1;
+  __syncthreads();
+  if ((n & 1) && inb && gl == 0) {
+    if (!(nx > 0.0)) flag[2] = 2 * grp;
+    if (!(ny > 0.0)) flag[2] = 2 * grp + 1;
+  }
+  __syncthreads();
+  const int zpos = flag[2];
+  if (inb) {
+#pragma unroll
+    for (int sl = 0; sl < 2; ++sl) {
+      int pos = 2 * grp + sl;
+      if ((n & 1) && pos == zpos) continue;      // the padding column
+      if (pos >= n) pos = zpos;                  // the column at position n
+      if (pos < 0 || pos >= n) continue;
+#pragma unroll
+      for (int t = 0; t < E; ++t) {
+        const int r = gl + G * t;
+        if (r < n) B[(long)pos * ldb + r] = sl ? y[t] : x[t];
+      }
+    }
+  }
+  __syncthreads();
+  return sweep >= maxsw ? SBLETKF_ERR_EIG_NOCONV : 0;
+}
+
 // Eigenpairs of the SPD matrix in B: eigenvectors replace B's columns and
 // lam[] receives the eigenvalues.  vec: n doubles, perm: n ints of scratch;
 // flag: >= 4 shared ints (flag[3] = sweeps run).  Returns status bits.
@@ -383,11 +551,11 @@ static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, doub
                                                  int *flag, int *perm, double *vec) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int bits = chol_pivot(B, n, ldb, perm, vec, flag);
-  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps<8>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, maxsw, vec, flag);
-  else bits |= jacobi_sweeps<EMAX>(B, n, ldb, tol, maxsw, vec, flag);
+  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps_oe<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps_oe<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, maxsw, vec, flag);
+  else bits |= jacobi_sweeps_oe<EMAX>(B, n, ldb, tol, maxsw, vec, flag);
   // lambda_j = |column j|^2; eigenvector = column / |column|, rows un-permuted
   for (int j = wid; j < n; j += nw) {
     double *cj = B + (long)j * ldb;
@@ -449,11 +617,11 @@ static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb,
   for (int e = tid; e < n * n; e += nt) B[(long)(e / n) * ldb + (e % n)] = X[e];
   __syncthreads();
   int bits = 0;
-  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps<8>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, maxsw, vec, flag);
-  else bits |= jacobi_sweeps<EMAX>(B, n, ldb, tol, maxsw, vec, flag);
+  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps_oe<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, maxsw, vec, flag);
+  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps_oe<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, maxsw, vec, flag);
+  else bits |= jacobi_sweeps_oe<EMAX>(B, n, ldb, tol, maxsw, vec, flag);
   for (int j = wid; j < n; j += nw) {
     double *cj = B + (long)j * ldb;
     double v[4], s = 0.0;
