@@ -6,9 +6,10 @@
 //                      log-likelihood (common_lpfgm.f90:64-69) in obs order
 //   jacobi_eig         eigenpairs of the SPD k x k matrix A = G + (k-1)/rho I
 //                      (replaces mtx_eigen / DSYEV, common.f90:992-1050):
-//                      one-sided (Hestenes) cyclic Jacobi on A in shared memory,
-//                      round-robin parallel ordering.  B <- A V converges to
-//                      columns lambda_j v_j, so lambda_j = |b_j|, v_j = b_j/lambda_j.
+//                      pivoted Cholesky, then one-sided (Hestenes) cyclic
+//                      Jacobi on the factor's columns, odd-even ordering
+//   jacobi_eig_warm    the same from a nearby matrix's eigenvectors V:
+//                      one-sided Jacobi on A V, lambda_j = |column j|
 //   pf_weights         max-subtracted exp, normalise, cumulative sum (serial)
 //   resample_draw      SR/MR draw, inum search and diagonal-priority assignment
 //                      (common_lpfgm.f90:89-197)
@@ -199,17 +200,16 @@ __device__ __forceinline__ void store_gram(const PointSmem &S, int k, double alp
 //     on A^2, whose squared gaps near the alpha cluster need many more
 //     sweeps), and the pivoted factor's columns start nearly orthogonal.
 //
-// Jacobi detail: round-robin ordering; in each of the n2-1 rounds the n2/2
-// disjoint column pairs are processed at once, one 4-lane group per pair, 8
-// pairs per warp.  The stride ldb = 4 (mod 16) doubles puts the 8 groups'
-// 4-double segments of consecutive columns on disjoint banks.  Column norms
-// are carried in nrm[] (recomputed each sweep), so only b_p.b_q is a dot
-// product.  A pair is rotated when (b_p.b_q)^2 > tol^2 |b_p|^2 |b_q|^2; the
-// angle t is computed in FP32 while c = 1/sqrt(1+t^2), s = c t are FP64, so
-// every rotation is orthogonal to FP64 rounding and the angle only has to
-// shrink b_p.b_q (the residual of a rotation is ~1e-7 of what it removes).
-// A sweep whose largest relative b_p.b_q was below 1e-10 leaves the columns
-// orthogonal to working precision, so the loop ends after it.
+// Jacobi detail: odd-even ordering (jacobi_sweeps_oe below) with 4-lane
+// groups, each holding a column pair in registers and passing one column per
+// step to a neighbour through shared memory.  Column norms are carried
+// (recomputed each sweep), so only b_p.b_q is a dot product.  A pair is
+// rotated when (b_p.b_q)^2 > tol^2 |b_p|^2 |b_q|^2; the angle t is computed
+// in FP32 while c = 1/sqrt(1+t^2), s = c t are FP64, so every rotation is
+// orthogonal to FP64 rounding and the angle only has to shrink b_p.b_q (the
+// residual of a rotation is ~1e-7 of what it removes).  A sweep whose largest
+// relative b_p.b_q was below 1e-10 leaves the columns orthogonal to working
+// precision, so the loop ends after it.
 // ---------------------------------------------------------------------------
 
 // In-place pivoted Cholesky of the full symmetric matrix in B: on return B's
@@ -290,92 +290,7 @@ static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *pe
   return flag[1];
 }
 
-// Jacobi sweeps on the columns of B (shared memory); E = elements per lane
-// (n <= 4E).  nrm: n doubles of scratch.  flag: >= 3 shared ints.
-template <int E>
-static __device__ __forceinline__ int jacobi_sweeps(double *B, int n, int ldb, double tol, int maxsw, double *nrm,
-                                                    int *flag) {
-  constexpr int G = 4;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int grp = lane / G, gl = lane % G, lead = grp * G;
-  const int n2 = (n + 1) & ~1, m = n2 - 1, npair = n2 / 2;
-  const double tol2 = tol * tol, big2 = 1e-20;
-  int sweep = 0;
-  for (; sweep < maxsw; ++sweep) {
-    for (int j = wid; j < n; j += nw) {  // exact column norms at the start of a sweep
-      const double *cj = B + (long)j * ldb;
-      double s = 0.0;
-      for (int r = lane; r < n; r += 32) s = fma(cj[r], cj[r], s);
-      s = __shfl_sync(0xffffffffu, warp_sum(s), 0);
-      if (lane == 0) nrm[j] = s;
-    }
-    if (threadIdx.x == 0) *flag = 0;
-    __syncthreads();
-    for (int rd = 0; rd < m; ++rd) {
-      for (int base = wid * (32 / G); base < npair; base += nw * (32 / G)) {
-        const int pi = base + grp;
-        int a = 0, b = 0;
-        if (pi == 0) {
-          a = m;
-          b = rd;
-        } else {
-          a = rd + pi;
-          if (a >= m) a -= m;
-          b = rd - pi;
-          if (b < 0) b += m;
-        }
-        const bool act = pi < npair && a < n && b < n;
-        double *ca = B + (long)(act ? a : 0) * ldb, *cb = B + (long)(act ? b : 0) * ldb;
-        double va[E], vb[E], g0 = 0.0, g1 = 0.0;
-#pragma unroll
-        for (int t = 0; t < E; ++t) {
-          const int r = gl + G * t;
-          const bool in = act && r < n;
-          va[t] = in ? ca[r] : 0.0;
-          vb[t] = in ? cb[r] : 0.0;
-          if (t & 1) g1 = fma(va[t], vb[t], g1);
-          else g0 = fma(va[t], vb[t], g0);
-        }
-        double ga = g0 + g1;
-#pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) ga += __shfl_xor_sync(0xffffffffu, ga, o);
-        // one value per group, so every lane of a pair applies the same rotation
-        ga = __shfl_sync(0xffffffffu, ga, lead);
-        const double al = act ? nrm[a] : 1.0, be = act ? nrm[b] : 1.0;
-        const double g2 = ga * ga, ab = al * be;
-        if (act && g2 > tol2 * ab) {
-          const float zf = __fdividef((float)(be - al) * 0.5f, (float)ga);
-          const float tf = copysignf(1.0f, zf) / (fabsf(zf) + sqrtf(fmaf(zf, zf, 1.0f)));
-          const double tt = (double)tf;
-          const double cs = rsqrt(fma(tt, tt, 1.0)), sn = cs * tt;
-#pragma unroll
-          for (int t = 0; t < E; ++t) {
-            const int r = gl + G * t;
-            if (r < n) {
-              ca[r] = cs * va[t] - sn * vb[t];
-              cb[r] = sn * va[t] + cs * vb[t];
-            }
-          }
-          if (gl == 0) {
-            const double c2 = cs * cs, s2 = sn * sn, csg = 2.0 * cs * sn * ga;
-            nrm[a] = c2 * al - csg + s2 * be;
-            nrm[b] = s2 * al + csg + c2 * be;
-            if (g2 > big2 * ab) *flag = 1;
-          }
-        }
-      }
-      __syncthreads();
-    }
-    const int rot = *flag;
-    __syncthreads();
-    if (!rot) break;
-  }
-  if (threadIdx.x == 0) flag[3] = sweep;  // sweeps run (diagnostics)
-  __syncthreads();
-  return sweep >= maxsw ? SBLETKF_ERR_EIG_NOCONV : 0;
-}
-
-// The same one-sided sweeps with the odd-even ordering, columns held in
+// One-sided Jacobi sweeps with the odd-even ordering, columns held in
 // registers: 4-lane group g holds the columns at positions (2g, 2g+1) in odd
 // steps and (2g+1, 2g+2) in even steps (E rows per lane each).  After a
 // rotation the pair's columns trade positions, so after an odd step a group
