@@ -193,8 +193,11 @@ def cpu_baseline(case, p, seconds: float = 15.0, nthreads: int = 0, uniforms=Non
                       f"C/OpenMP restatement, r_size=binary32 (reference default build), {dt:.1f} s"}
 
 
-def scaled_workload(wl, s: int):
-    """The workload with nlon, nlat / s and observation counts / s^2."""
+def scaled_workload(wl, s: int, levels: int = 0):
+    """The workload with nlon, nlat / s and observation counts / s^2, and
+    with `levels` vertical levels when levels > 0."""
+    if levels > 0:
+        wl = wl.scaled(nlev=levels, name=wl.name + f" ({levels} levels)")
     if s <= 1:
         return wl
     q = s * s
@@ -255,7 +258,7 @@ def reference_arm(args, rank, world):
     if rank != 0:
         return
     dev = "cuda:0" if torch.cuda.is_available() else "cpu"
-    wl = scaled_workload(WORKLOADS[args.workload], args.scale)
+    wl = scaled_workload(WORKLOADS[args.workload], args.scale, args.levels)
     case = make_case(wl, device=dev, seed=wl.seed)
     p = case.params.replace(precision=0)
     uni = None
@@ -302,6 +305,9 @@ def main():
     ap.add_argument("--scale", type=int, default=1,
                     help="divide nlon and nlat by S and the obs counts by S^2 (same obs density; "
                          "for profiling runs)")
+    ap.add_argument("--levels", type=int, default=0,
+                    help="use L vertical levels instead of the workload's (for profiling runs: the full "
+                         "horizontal grid, so the same column-queue items, at a fraction of the points)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -329,7 +335,7 @@ def main():
 
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
-    wl = scaled_workload(WORKLOADS[args.workload], args.scale)
+    wl = scaled_workload(WORKLOADS[args.workload], args.scale, args.levels)
     case = make_case(wl, device=dev, seed=wl.seed + rank)
     prec = PREC_MIXED if args.precision == "mixed" else PREC_FP64
     p = case.params.replace(precision=prec)
@@ -511,11 +517,12 @@ def main():
                     "note": "fused kernel: weights, nmonte draws and gather in one launch"}
         else:
             achieved = fl["total"] / (kern_ms / 1e3) / 1e12
-            # DRAM bytes per launch: ncu capture of the same kernel on the 1/8 grid
-            # (profiles/analysis_mixed_workload1_scale8_full.md), 274.7 MB for
-            # 74,000 points, scaled by the points of this launch
-            traffic = (274.7e6 / 74000.0 * P if (args.workload == 1 and prec == PREC_MIXED
-                                                 and args.schedule == "columns") else None)
+            # DRAM bytes per launch: ncu capture of the same kernel on the full
+            # horizontal grid with 2 levels, which gets the same 8-column queue
+            # items (profiles/analysis_mixed_workload1_scale8_full.md), 1309.3 MB
+            # for 240,000 points, scaled by the points of this launch
+            traffic = (1309.3e6 / 240000.0 * P if (args.workload == 1 and prec == PREC_MIXED
+                                                   and args.schedule == "columns") else None)
             roof = {"bound": "fp64", "achieved": achieved, "peak": f64["tflops"], "unit": "TFLOP/s",
                     "frac": achieved / f64["tflops"], "traffic": traffic, "kernel": "k_analysis",
                     "peak_source": f64["source"], "kernel_ms": kern_ms, "flops_per_launch": fl,

@@ -626,8 +626,9 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
 }
 
 // One CTA per grid point (queue == nullptr; point p0 + blockIdx.x), or a
-// persistent launch of one CTA per SM taking chunks of adjacent grid columns
-// from the atomic counter *queue and analysing their levels in snake order,
+// persistent launch of one CTA per SM taking items of up to colchunk grid
+// columns, cstride apart, from the atomic counter *queue and analysing their
+// levels in snake order,
 // warm-starting every primal eigensolve from the previous primal point
 // (slab: 2 k x k FP64 scratch matrices per CTA).
 template <int R, typename ST, bool MIXED>
@@ -635,7 +636,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_analysis(const sbletkf_params p, const GridView g, const ObsView ob, const ST *__restrict__ f3,
                const ST *__restrict__ f2, ST *__restrict__ a3, ST *__restrict__ a2, const double *__restrict__ uni,
                int32_t *__restrict__ src_out, int32_t *__restrict__ pst, int *status, long long p0, int *queue,
-               double *slab) {
+               double *slab, int colchunk, int cstride) {
   constexpr int KP = kp_of_r(R);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PointSmem S;
@@ -672,39 +673,39 @@ __global__ void __launch_bounds__(kThreads, 1)
     tcs.tbase = s_tmem;
   }
   // one call site of the point body for both schedules.  Column schedule: a
-  // queue item is kColChunk adjacent columns, walked in snake order (levels
-  // down, then up, ...), so every column's first level with a primal
-  // eigensolve starts from the same level of the column beside it and every
-  // later level from the level above or below.
-  constexpr int kColChunk = 8;
+  // queue item is up to colchunk (1..8) columns cstride apart -- with cstride
+  // = nlon, neighbours along a meridian -- walked in snake order (levels down,
+  // then up, ...), so every column's first level with a primal eigensolve
+  // starts from the same level of the column beside it and every later level
+  // from the level above or below.  Items q and q+1 hold adjacent columns of
+  // the same latitude rows, so the CTAs running at the same time read and
+  // write the same 32-byte sectors of the state at about the same time.
   double *vprev = queue ? slab + (size_t)blockIdx.x * 2 * k * k : nullptr;
   double *xtmp = queue ? vprev + (size_t)k * k : nullptr;
   __shared__ int s_item;
-  int warm = 0, col = 0, cend = 0, kl = 0, step = 1, remaining = 0;
+  int warm = 0, c0 = 0, w = 0, pos = 0, npos = 0;
   bool first = true;
   for (;;) {
     long long pid;
     if (queue) {
-      if (remaining == 0) {  // next column
-        ++col;
-        if (col >= cend) {   // next chunk of columns from the queue
-          if (tid == 0) s_item = atomicAdd(queue, 1);
-          __syncthreads();
-          const long long c0 = (long long)s_item * kColChunk;
-          __syncthreads();
-          if (c0 >= g.nij1) break;
-          col = (int)c0;
-          cend = (int)(c0 + kColChunk < g.nij1 ? c0 + kColChunk : g.nij1);
-          warm = 0;
-          step = 1;
-        }
-        step = -step;        // surface-down first, then bottom-up, ...
-        kl = step < 0 ? p.nlev - 1 : 0;
-        remaining = p.nlev;
+      if (pos == npos) {  // next item from the queue
+        if (tid == 0) s_item = atomicAdd(queue, 1);
+        __syncthreads();
+        const long long q = s_item, band = q / cstride;
+        const long long cs = band * colchunk * cstride + (q - band * cstride);
+        __syncthreads();
+        if (cs >= g.nij1) break;  // later items start further on
+        const long long left = (g.nij1 - cs + cstride - 1) / cstride;
+        c0 = (int)cs;
+        w = (int)(left < colchunk ? left : colchunk);
+        pos = 0;
+        npos = w * p.nlev;
+        warm = 0;
       }
-      pid = (long long)kl * g.nij1 + col;
-      kl += step;
-      --remaining;
+      const int j = pos / p.nlev, r = pos - j * p.nlev;
+      const int kl = (j & 1) ? r : p.nlev - 1 - r;  // surface-down first, then bottom-up, ...
+      ++pos;
+      pid = (long long)kl * g.nij1 + c0 + (long long)j * cstride;
     } else {
       if (!first) break;
       first = false;
@@ -765,10 +766,16 @@ int launch_r(const sbletkf_params *p, const GridView &g, const ObsView &ob, cons
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_status(e);
   if (sc.queue) {
+    // Queue items of up to 8 columns; narrower when the grid has fewer than
+    // 32 items of 8 per CTA, because the dynamic queue balances the CTAs'
+    // loads only to within about one item.
+    const long long per = (long long)g.nij1 / ((long long)sc.ctas * 32);
+    const int colchunk = per >= 8 ? 8 : per < 1 ? 1 : (int)per;
+    const int cstride = p->nlon > 1 ? p->nlon : 1;
     e = cudaMemsetAsync(sc.queue, 0, sizeof(int), s);
     if (e != cudaSuccess) return cuda_status(e);
     kern<<<(unsigned)sc.ctas, kThreads, smem, s>>>(*p, g, ob, (const ST *)f3, (const ST *)f2, (ST *)a3, (ST *)a2,
-                                                    uni, src, pst, status, 0, sc.queue, sc.slab);
+                                                    uni, src, pst, status, 0, sc.queue, sc.slab, colchunk, cstride);
     return cuda_status(cudaGetLastError());
   }
   const long long P = (long long)p->nlev * g.nij1;
@@ -776,7 +783,7 @@ int launch_r(const sbletkf_params *p, const GridView &g, const ObsView &ob, cons
   for (long long p0 = 0; p0 < P; p0 += maxg) {
     const long long n = P - p0 < maxg ? P - p0 : maxg;
     kern<<<(unsigned)n, kThreads, smem, s>>>(*p, g, ob, (const ST *)f3, (const ST *)f2, (ST *)a3, (ST *)a2, uni,
-                                              src, pst, status, p0, nullptr, nullptr);
+                                              src, pst, status, p0, nullptr, nullptr, 1, 1);
   }
   return cuda_status(cudaGetLastError());
 }
