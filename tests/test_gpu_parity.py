@@ -213,3 +213,32 @@ def test_both_schedules_match_the_oracle(k, precision, cuda):
         assert field_relerr(r["anal2d"], ref["anal2d"]) <= tol
     # warm and cold eigensolves round differently: far below the 1e-10 parity bound
     assert field_relerr(r1["anal3d"], r0["anal3d"]) <= (1e-11 if precision == 0 else 1e-6)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_column_queue_with_multi_column_items(precision, cuda):
+    """A grid wide enough that the column queue hands out items of several
+    columns one latitude row apart (38,400 columns: 8 per item on a 148-SM
+    B200, at least 2 on any GPU with up to 600 SMs).  Outputs start as NaN, so
+    a point that no item covers fails the comparison with the oracle."""
+    wl = WORKLOADS[0].scaled(nlon=400, nlat=96, nlev=3, nmem=20, n_sst=6000, n_ssh=2000, n_prof=30,
+                             lat0=-12.0, seed=515)
+    case = make_case(wl, cov_infl_mul=1.1, alpha_rtps=0.4)
+    g, ob, f3, f2 = _np(case)
+    ref = cref.da_main(case.params, g, ob, f3, f2, rsize=8)
+    p = case.params.replace(precision=precision)
+    dev = "cuda:0"
+    an = Analysis(p, case.nij1, ob["elm"].size, device=dev)
+    an.set_schedule(Analysis.SCHED_COLUMNS)
+    an.prepare_obs({k: torch.as_tensor(v, device=dev) for k, v in ob.items()})
+    gt = {k: torch.as_tensor(v, device=dev, dtype=torch.float64) for k, v in g.items()}
+    a3 = torch.full(f3.shape, float("nan"), dtype=torch.float64, device=dev)
+    a2 = torch.full(f2.shape, float("nan"), dtype=torch.float64, device=dev)
+    an.da_main(gt, torch.as_tensor(f3, device=dev, dtype=torch.float64),
+               torch.as_tensor(f2, device=dev, dtype=torch.float64), anal3d=a3, anal2d=a2)
+    an.close()
+    r3, r2 = a3.cpu().numpy(), a2.cpu().numpy()
+    assert not np.isnan(r3).any() and not np.isnan(r2).any()
+    tol = TOL64 if precision == 0 else TOL_MIXED
+    assert field_relerr(r3, ref["anal3d"]) <= tol
+    assert field_relerr(r2, ref["anal2d"]) <= tol
