@@ -28,11 +28,11 @@ struct TcState {
   uint32_t tbase;   // TMEM base: sum hi, sum lo, chunk accumulators 0 and 1 (KP columns each)
   int uses[2];      // commits issued per operand stage
   int nchunk;
-  int nflushed;     // chunks added into the running sum
+  int nflushed;     // chunk pairs added into the running sum
   int broken;       // a wait timed out: issue nothing more
 };
 
-// Add the chunk accumulator of stage s into the running double-FP32 sum with
+// Add chunk accumulator a (0, 1) into the running double-FP32 sum with
 // Knuth's TwoSum (hi + c = s_ + e exactly; lo += e).  Whole CTA: warp w owns
 // TMEM lanes 32 (w % 4) .. +31 and half w / 4 of the 16-column groups.
 template <int KP>
@@ -73,8 +73,10 @@ __device__ __forceinline__ void tc_flush(TcState &st, int s) {
 }
 
 // Stage `cnt` list entries starting at f as BF16 h/m/l operand tiles and issue
-// their six UMMAs per K-block into the stage's chunk accumulator, after adding
-// that accumulator's previous chunk into the running sum.  Also
+// their six UMMAs per K-block.  Chunks 2p and 2p+1 share chunk accumulator
+// p % 2 (FP32 over 128 observations); at chunk 2p+3, whose entry wait on
+// stage 1 covers chunk 2p+1's UMMAs, pair p is added into the running sum,
+// before chunk 2p+4 starts that accumulator afresh.  Also
 // accumulates b = sum w dep y (FP64) and, when do_pf, the PF log-likelihood.
 // Whole CTA; ends with the tiles handed to the tensor core.
 template <int KP>
@@ -107,9 +109,9 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
   if (tid < kKC) sw[tid] = tid < cnt ? (float)sqrt(S.lw[f + tid]) : 0.0f;
   __syncthreads();
   st.broken = s_broken;
-  if (!st.broken && st.nchunk >= 2) {  // this point's chunk two back is complete: add it to the sum
+  if (!st.broken && (st.nchunk & 1) && st.nchunk >= 3) {  // pair (nchunk - 3) / 2 is complete: add it
     fence_after_sync();
-    tc_flush<KP>(st, s);
+    tc_flush<KP>(st, ((st.nchunk >> 1) + 1) & 1);
     fence_before_sync();
   }
   if (tid < KP)
@@ -142,8 +144,8 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
     for (int kb = 0; kb < kKC / kKB; ++kb) {
       const uint64_t dh = sdesc(a0 + kb * kBlockBytes), dm = sdesc(a0 + kTileBytes + kb * kBlockBytes),
                      dl = sdesc(a0 + 2 * kTileBytes + kb * kBlockBytes);
-      const uint32_t acc = kb > 0 ? 1u : 0u;   // each chunk starts a fresh accumulator
-      const uint32_t d = st.tbase + (uint32_t)((2 + s) * KP);
+      const uint32_t acc = (kb > 0 || (st.nchunk & 1)) ? 1u : 0u;  // each pair starts a fresh accumulator
+      const uint32_t d = st.tbase + (uint32_t)((2 + ((st.nchunk >> 1) & 1)) * KP);
       mma_bf16(d, dh, dh, idesc, acc);  // H^T H
       mma_bf16(d, dh, dm, idesc, 1u);   // H^T M
       mma_bf16(d, dm, dh, idesc, 1u);   // M^T H
@@ -157,7 +159,8 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, 
   st.nchunk++;
 }
 
-// Wait for every issued UMMA, add the last chunks into the running sum, then
+// Wait for every issued UMMA, add the pairs not yet flushed (at most two) into
+// the running sum, then
 // G + alpha I = hi + lo + alpha I into B (FP64, column-major, stride ldb; the
 // lower triangle read and mirrored, so B is exactly symmetric) and b into S.b.
 template <int KP>
@@ -179,8 +182,7 @@ __device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint6
   st.broken = s_brk;
   fence_after_sync();
   if (!st.broken)
-    for (int t = st.nchunk - 2; t < st.nchunk; ++t)
-      if (t >= 0) tc_flush<KP>(st, t & 1);
+    for (int pr = st.nflushed; pr <= ((st.nchunk - 1) >> 1); ++pr) tc_flush<KP>(st, pr & 1);
   double *B = S.u;
   const int q = wid & 3, half = wid >> 2, r = 32 * q + lane;
   const uint32_t trow = st.tbase + ((uint32_t)(32 * q) << 16);

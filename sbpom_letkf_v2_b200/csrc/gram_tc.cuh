@@ -8,11 +8,11 @@
 // six UMMAs per K-block into an FP32 chunk accumulator in tensor memory; the
 // dropped terms (M^T L, L^T M, L^T L) are below 2^-24 of G.  Transposed pairs
 // are separate UMMAs (A and B swapped), so the accumulator needs no transpose.
-// Each chunk (64 observations) has its own accumulator, which the CTA adds
-// into a running double-FP32 sum (hi + lo, error-free TwoSum) also held in
-// tensor memory, so FP32 rounding stays at the scale of one chunk rather than
-// growing with nobsl.  Tensor-memory columns: sum hi [0,KP), sum lo [KP,2KP),
-// chunk accumulators of the two operand stages [2KP,3KP) and [3KP,4KP).
+// Each pair of chunks (2 x 64 observations) has its own accumulator, which
+// the CTA adds into a running double-FP32 sum (hi + lo, error-free TwoSum)
+// also held in tensor memory, so FP32 rounding stays at the scale of one
+// chunk pair rather than growing with nobsl.  Tensor-memory columns: sum hi
+// [0,KP), sum lo [KP,2KP), chunk-pair accumulators [2KP,3KP) and [3KP,4KP).
 // (common_letkf.f90:93-122 computes the same Gram with sgemm/dgemm.)
 //
 // Operand tile: rows = members (M = 128, zero-padded), K = observations, in the
