@@ -519,9 +519,9 @@ def main():
             achieved = fl["total"] / (kern_ms / 1e3) / 1e12
             # DRAM bytes per launch: ncu capture of the same kernel on the full
             # horizontal grid with 2 levels, which gets the same 8-column queue
-            # items (profiles/analysis_mixed_workload1_scale8_full.md), 1309.3 MB
+            # items (profiles/analysis_mixed_workload1_scale8_full.md), 1073.6 MB
             # for 240,000 points, scaled by the points of this launch
-            traffic = (1309.3e6 / 240000.0 * P if (args.workload == 1 and prec == PREC_MIXED
+            traffic = (1073.6e6 / 240000.0 * P if (args.workload == 1 and prec == PREC_MIXED
                                                    and args.schedule == "columns") else None)
             roof = {"bound": "fp64", "achieved": achieved, "peak": f64["tflops"], "unit": "TFLOP/s",
                     "frac": achieved / f64["tflops"], "traffic": traffic, "kernel": "k_analysis",
