@@ -1,0 +1,81 @@
+"""Host-side pieces of bench.py on the CPU: workload scaling for profiling
+runs, the algorithmic work formulas behind `roofline`, the mixed-path error
+metric, and the JSON line of the reference arm (the CPU restatement timed
+on a column sample)."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import torch
+
+import bench
+from sbpom_letkf_v2_b200.synthetic import WORKLOADS
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_scaled_workload_grid_levels_and_obs_density():
+    wl = WORKLOADS[1]
+    assert bench.scaled_workload(wl, 1) is wl
+    s8 = bench.scaled_workload(wl, 8)
+    assert (s8.nlon, s8.nlat, s8.nlev) == (50, 37, 40)
+    assert (s8.n_sst, s8.n_ssh, s8.n_prof) == (wl.n_sst // 64, wl.n_ssh // 64, wl.n_prof // 64)
+    l2 = bench.scaled_workload(wl, 1, levels=2)
+    assert (l2.nlon, l2.nlat, l2.nlev) == (400, 300, 2)
+    assert (l2.n_sst, l2.n_ssh, l2.n_prof) == (wl.n_sst, wl.n_ssh, wl.n_prof)   # full horizontal grid
+    both = bench.scaled_workload(wl, 4, levels=3)
+    assert (both.nlon, both.nlat, both.nlev) == (100, 75, 3)
+
+
+def test_algorithmic_work_formulas():
+    """Per point with n local obs: F_gram = 2k^2 n, F_eig = 9k^3 and
+    F_W = 2k^3 + 2kn + 2k^2 only where n > 0, F_upd = 2 nv k^2; bytes
+    B_w = 4n(k+3), B_g = 8 k nv; nv includes the 2D variables on the
+    surface level (the last one)."""
+    k, nv3d, nv2d, nlev, nij1 = 10, 4, 1, 2, 3
+    n = np.array([0, 5, 7, 1, 0, 2], dtype=np.int64)        # [nlev][nij1]
+    f = bench.algorithmic_flops(n, k, nv3d, nv2d, nlev, nij1)
+    has = (n > 0).sum()
+    nv = np.array([nv3d] * nij1 + [nv3d + nv2d] * nij1, dtype=np.float64)
+    assert f["gram"] == 2.0 * k * k * n.sum()
+    assert f["eig"] == 9.0 * k ** 3 * has
+    assert f["w"] == float(((2.0 * k ** 3 + 2.0 * k * n + 2.0 * k * k) * (n > 0)).sum())
+    assert f["upd"] == float((2.0 * nv * k * k).sum())
+    assert f["total"] == f["gram"] + f["eig"] + f["w"] + f["upd"]
+    b = bench.algorithmic_bytes(n, k, nv3d, nv2d, nlev, nij1)
+    assert b["weights"] == float((4.0 * n * (k + 3)).sum())
+    assert b["gather"] == float((8.0 * k * nv).sum())
+
+
+def test_mean_spread_error_metric():
+    g = torch.Generator().manual_seed(4)
+    r3 = torch.randn(2, 16, 3, 5, generator=g, dtype=torch.float64) + 10.0
+    r2 = torch.randn(1, 16, 5, generator=g, dtype=torch.float64)
+    z = bench.mean_spread_error(r3, r2, r3, r2)
+    assert z == {"mean_max": 0.0, "mean_rms": 0.0, "spread_max": 0.0, "spread_rms": 0.0}
+    a3 = r3.clone()
+    a3[1] += 1e-3                                            # shifts variable 1's mean only
+    e = bench.mean_spread_error(a3, r2, r3, r2)
+    want = 1e-3 / float(r3[1].mean(0).abs().max())
+    # the shift itself rounds at eps * 10 / 1e-3 ~ 2e-12 relative
+    assert abs(e["mean_max"] - want) <= 1e-9 * want
+    assert e["spread_max"] < 1e-12
+
+
+def test_reference_arm_json_line():
+    """`bench.py --impl reference` prints one JSON line with the contract's
+    keys; its e2e moves no bytes between host and device."""
+    r = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--workload", "0", "--steps", "1",
+                        "--warmup", "0", "--ref-seconds", "0.5"], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["unit"] == "gridpoints/s" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    assert line["config"]["workload"] == WORKLOADS[0].name
