@@ -96,20 +96,23 @@ __global__ void __launch_bounds__(kThreads, 1)
       __syncthreads();
       pf_weights(S, k);
       int16_t *srcb = reinterpret_cast<int16_t *>(S.u);
-      uint8_t *hist = reinterpret_cast<uint8_t *>(srcb + kDrawBatch * k);
+      const int wid = tid >> 5, lane = tid & 31;
+      int *whist = reinterpret_cast<int *>(srcb + kDrawBatch * k) + wid * k;
+      int16_t *wup =
+          reinterpret_cast<int16_t *>(reinterpret_cast<int *>(srcb + kDrawBatch * k) + (kThreads / 32) * k) + wid * k;
       uint16_t *cnt = reinterpret_cast<uint16_t *>(S.x);  // [member j][particle i]
       for (int e = tid; e < k * k; e += kThreads) cnt[e] = 0;
       for (int d0 = 0; d0 < p.nmonte; d0 += kDrawBatch) {
         const int nb = min(kDrawBatch, p.nmonte - d0);
         __syncthreads();
-        if (tid < nb) {
-          const int d = d0 + tid;
+        for (int t = wid; t < nb; t += kThreads / 32) {  // a warp per draw
+          const int d = d0 + t;
           const double *u = (p.rm == SBLETKF_RM_SR) ? uni + q * p.nmonte + d : uni + (q * p.nmonte + d) * k;
-          int16_t *sr = srcb + tid * k;
-          resample_draw(p, S.cw, k, u, hist + tid * k, sr);
+          int16_t *sr = srcb + t * k;
+          resample_draw(p, S.cw, k, u, whist, wup, sr);
           if (src_out) {
             int32_t *so = src_out + (q * p.nmonte + d) * k;
-            for (int j = 0; j < k; ++j) so[j] = sr[j];
+            for (int j = lane; j < k; j += 32) so[j] = sr[j];
           }
         }
         __syncthreads();

@@ -11,7 +11,7 @@
 //   jacobi_eig_warm    the same from a nearby matrix's eigenvectors V:
 //                      one-sided Jacobi on A V, lambda_j = |column j|
 //   pf_weights         max-subtracted exp, normalise, cumulative sum (serial)
-//   resample_draw      SR/MR draw, inum search and diagonal-priority assignment
+//   resample_draw      SR/MR draw, inum search and diagonal-priority assignment (one warp)
 //                      (common_lpfgm.f90:89-197)
 #pragma once
 
@@ -25,6 +25,12 @@ __host__ __device__ constexpr int kp_of_r(int r) { return 16 * r; }
 inline int r_for_k(int k) { return k <= 32 ? 2 : k <= 64 ? 4 : k <= 112 ? 7 : 8; }
 
 constexpr int kDrawBatch = 64;  // PF draws resolved per pass
+
+// Shared memory of the PF draws: kDrawBatch draws' src rows (int16), then per
+// warp a k-int histogram and k int16 unused-column ranks.
+__host__ __device__ constexpr size_t pf_draw_bytes(int k) {
+  return (size_t)kDrawBatch * k * sizeof(int16_t) + (size_t)(kThreads / 32) * k * (sizeof(int) + sizeof(int16_t));
+}
 // Leading dimension of an n x n eigensolver matrix: 4 (mod 16) doubles.
 __host__ __device__ inline int eig_ld(int n) { return (n + 15) / 16 * 16 + 4; }
 
@@ -55,7 +61,7 @@ struct PointSmem {
     const size_t kk = (size_t)k;
     size_t mat = sizeof(double) * kk * eig_ld(kp);
     size_t dual = sizeof(double) * (nd * (kp + 1) + nd * eig_ld((int)nd));
-    size_t pf = (size_t)kDrawBatch * k * (sizeof(int16_t) + 1) + 16;
+    size_t pf = pf_draw_bytes(k) + 16;
     size_t m = chunk > mat ? chunk : mat;
     m = m > dual ? m : dual;
     m = m > tcb ? m : tcb;
@@ -638,43 +644,64 @@ __device__ __forceinline__ int pf_select(const double *cw, int k, double r) {
   return lo;
 }
 
-// One resampling draw (common_lpfgm.f90:89-197) by one thread.
-// hist: k bytes of scratch.  src[j] = particle (0-based) taken by member j.
-// The selected particles depend on the uniforms only through the histogram of
-// inum (inum is monotone in the sorted uniforms), so SR and MR share the
-// assignment below; MR needs no sort.
+// One resampling draw (common_lpfgm.f90:89-197) by one warp, k <= 128.
+// hist: k ints, upos: k int16 of this warp's scratch.  src[j] = particle
+// (0-based) taken by member j.  The selected particles depend on the uniforms
+// only through the histogram of inum (inum is monotone in the sorted
+// uniforms), so SR and MR share the assignment below; MR needs no sort.  SR:
+// the reference's r_j (same operations) ascend, so its merge scan finds for
+// each j the first i with r_j <= cw(i) (capped at k-1) -- what pf_select
+// returns -- and lanes search independently.  Diagonal priority: every
+// selected particle keeps its own column; the extra copies, in increasing
+// particle order, take the unused columns in increasing order (:152-181),
+// i.e. extra copy number e goes to unused column number e, both ranked by
+// warp prefix sums.
 __device__ __forceinline__ void resample_draw(const sbletkf_params &p, const double *cw, int k, const double *u,
-                                              uint8_t *hist, int16_t *src) {
-  for (int i = 0; i < k; ++i) hist[i] = 0;
+                                              int *hist, int16_t *upos, int16_t *src) {
+  constexpr int PL = 4;  // particles per lane: i = PL lane .. PL lane + 3
+  const int lane = threadIdx.x & 31;
+  for (int i = lane; i < k; i += 32) hist[i] = 0;
+  __syncwarp();
   if (p.rm == SBLETKF_RM_SR) {
     const double r1 = __ddiv_rn(__dsub_rn(__dadd_rn(u[0], 1.0), 1.0), (double)k);
     const double base = p.sr_textbook ? u[0] : r1;
-    int i = 0;
-    for (int j = 0; j < k; ++j) {
+    for (int j = lane; j < k; j += 32) {
       const double r = j == 0 ? r1 : __ddiv_rn(__dsub_rn(__dadd_rn(base, (double)(j + 1)), 1.0), (double)k);
-      while (i < k - 1 && !(r <= cw[i])) ++i;  // r ascending -> merge scan
-      hist[i]++;
+      atomicAdd(&hist[pf_select(cw, k, r)], 1);
     }
   } else {
-    for (int j = 0; j < k; ++j) hist[pf_select(cw, k, u[j])]++;
+    for (int j = lane; j < k; j += 32) atomicAdd(&hist[pf_select(cw, k, u[j])], 1);
+  }
+  __syncwarp();
+  int cnt[PL], nun = 0, nex = 0, nall = 0;
+#pragma unroll
+  for (int t = 0; t < PL; ++t) {
+    const int i = PL * lane + t;
+    cnt[t] = i < k ? hist[i] : 0;
+    nun += (i < k && cnt[t] == 0) ? 1 : 0;
+    nex += cnt[t] > 1 ? cnt[t] - 1 : 0;
+    nall += cnt[t];
   }
   if (p.dp) {
-    // diagonal priority: every selected particle keeps its own column; the
-    // extra copies, in increasing particle order, fill the unused columns
-    // left to right (:152-181)
-    int f = 0;
-    for (int i = 0; i < k; ++i)
-      if (hist[i]) src[i] = (int16_t)i;
-    for (int i = 0; i < k; ++i)
-      for (int c = 1; c < hist[i]; ++c) {
-        while (f < k - 1 && hist[f]) ++f;
-        src[f++] = (int16_t)i;
-      }
+    int ru = warp_incl_scan(nun) - nun;  // rank of this lane's first unused column
+#pragma unroll
+    for (int t = 0; t < PL; ++t) {
+      const int i = PL * lane + t;
+      if (i < k && cnt[t] == 0) upos[ru++] = (int16_t)i;
+      if (cnt[t] > 0) src[i] = (int16_t)i;
+    }
+    __syncwarp();
+    int re = warp_incl_scan(nex) - nex;  // rank of this lane's first extra copy
+#pragma unroll
+    for (int t = 0; t < PL; ++t)
+      for (int c = 1; c < cnt[t]; ++c) src[upos[re++]] = (int16_t)(PL * lane + t);
   } else {
-    int j = 0;
-    for (int i = 0; i < k; ++i)
-      for (int c = 0; c < hist[i]; ++c) src[j++] = (int16_t)i;
+    int q = warp_incl_scan(nall) - nall;
+#pragma unroll
+    for (int t = 0; t < PL; ++t)
+      for (int c = 0; c < cnt[t]; ++c) src[q++] = (int16_t)(PL * lane + t);
   }
+  __syncwarp();
 }
 
 // Mean / spread (k-1) / perturbation of S.x rows v < nvt, warp v per row
