@@ -313,6 +313,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # host cores only: rank 0 runs, the other ranks exit; no process group
+        reference_arm(args, rank, world)
+        return
     pg = False
     if world > 1:
         import datetime
@@ -322,12 +326,6 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device(f"cuda:{local}"))
         pg = True
-    if args.impl == "reference":
-        reference_arm(args, rank, world)
-        if pg:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return
 
     from sbpom_letkf_v2_b200.analysis import Analysis
     from sbpom_letkf_v2_b200.params import PREC_FP64, PREC_MIXED
