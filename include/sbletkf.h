@@ -256,10 +256,12 @@ int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const vo
 
 /* Launch schedule of sbletkf_analysis for this workspace.
  * SBLETKF_SCHED_COLUMNS (the default, except for the LPF): one persistent CTA
- * per SM takes chunks of adjacent grid columns from an atomic queue and walks
- * their levels in snake order, starting every k x k eigensolve from the
- * eigenvectors of the previous one.  SBLETKF_SCHED_POINT (the LPF default,
- * which has no eigensolve): one CTA per grid point.  Both give the same analysis to rounding.
+ * per SM takes items of up to 8 grid columns, nlon apart (neighbours along a
+ * meridian), from an atomic queue and walks their levels in snake order,
+ * starting every k x k eigensolve from the eigenvectors of the previous one;
+ * items narrow to 1 column when the grid has fewer than 32 items of 8 per CTA.
+ * SBLETKF_SCHED_POINT (the LPF default, which has no eigensolve): one CTA per
+ * grid point.  Both give the same analysis to rounding.
  * No reference counterpart (the reference's OpenMP DYNAMIC loop over (k,i),
  * common_da.f90:66-68, is the scheduling it replaces). */
 #define SBLETKF_SCHED_POINT   0
