@@ -508,8 +508,12 @@ def main():
         if pf:
             by = algorithmic_bytes(nobsl, p.nmem, p.nv3d, p.nv2d, p.nlev, case.nij1)
             gbs = by["total"] / (kern_ms / 1e3) / 1e9
+            # DRAM bytes per launch: ncu capture of the same kernel on the 1/2
+            # grid of workload 4 (profiles/analysis_lpf_workload4_scale2.md),
+            # 280.6 MB for 61,440 points, scaled by the points of this launch
+            traffic = 280.6e6 / 61440.0 * P if args.workload == 4 else None
             roof = {"bound": "hbm", "achieved": gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                    "frac": gbs / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None, "traffic": None,
+                    "frac": gbs / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None, "traffic": traffic,
                     "kernel": "k_analysis (LPF weights + resampling gather)", "kernel_ms": kern_ms,
                     "bytes_per_launch": by, "peak_source": src + " hbm_gbs (copy)",
                     "note": "fused kernel: weights, nmonte draws and gather in one launch"}
