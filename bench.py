@@ -508,9 +508,9 @@ def main():
         if pf:
             by = algorithmic_bytes(nobsl, p.nmem, p.nv3d, p.nv2d, p.nlev, case.nij1)
             gbs = by["total"] / (kern_ms / 1e3) / 1e9
-            # DRAM bytes per launch: ncu capture of the same kernel on the 1/2
-            # grid of workload 4 (profiles/analysis_lpf_workload4_scale2.md),
-            # 280.6 MB for 61,440 points, scaled by the points of this launch
+            # DRAM bytes per launch: an ncu capture of the same kernel on the 1/2
+            # grid of workload 4 (bench.py --workload 4 --scale 2) read and
+            # wrote 280.6 MB for 61,440 points; scaled by the points of this launch
             traffic = 280.6e6 / 61440.0 * P if args.workload == 4 else None
             roof = {"bound": "hbm", "achieved": gbs, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                     "frac": gbs / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None, "traffic": traffic,
@@ -519,10 +519,10 @@ def main():
                     "note": "fused kernel: weights, nmonte draws and gather in one launch"}
         else:
             achieved = fl["total"] / (kern_ms / 1e3) / 1e12
-            # DRAM bytes per launch: ncu capture of the same kernel on the full
-            # horizontal grid with 2 levels, which gets the same 8-column queue
-            # items (profiles/analysis_mixed_workload1_scale8_full.md), 1073.6 MB
-            # for 240,000 points, scaled by the points of this launch
+            # DRAM bytes per launch: an ncu capture of the same kernel on the full
+            # horizontal grid with 2 levels (bench.py --levels 2), which gets the
+            # same 8-column queue items, read and wrote 1073.6 MB for 240,000
+            # points; scaled by the points of this launch
             traffic = (1073.6e6 / 240000.0 * P if (args.workload == 1 and prec == PREC_MIXED
                                                    and args.schedule == "columns") else None)
             roof = {"bound": "fp64", "achieved": achieved, "peak": f64["tflops"], "unit": "TFLOP/s",
