@@ -171,6 +171,13 @@ int sbletkf_count_nobsl(sbletkf_workspace *ws, const sbletkf_params *p,
 /* Synchronise `stream`, return and clear the latched device status. */
 int sbletkf_get_status(sbletkf_workspace *ws, void *stream, int32_t *status);
 
+/* OR `bits` into the workspace's latched device status, in stream order
+ * (asynchronous).  Host-side failure injection: a test latches
+ * SBLETKF_ERR_TIMEOUT before an analysis to drive the path every later launch
+ * takes after a tensor-core wait has expired (no tensor memory allocated, no
+ * UMMA issued, every point marked).  No reference counterpart. */
+int sbletkf_latch_status(sbletkf_workspace *ws, int32_t bits, void *stream);
+
 /* Ragged batch of per-point cores: letkf_core / letkf_core_noobs
  * (common_letkf.f90:37-210) or lpfgm_core / lpfgm_core_noobs
  * (common_lpfgm.f90:422-494) on npts independent local problems.
@@ -196,10 +203,17 @@ int sbletkf_core_batched(const sbletkf_params *p, int32_t npts, const int64_t *o
  * Limits: obs->nobs <= SBLETKF_NOALLOC_MAX_OBS, nlon*nlat <=
  * SBLETKF_NOALLOC_MAX_CELLS, nmem <= 128; larger calls return
  * SBLETKF_ERR_WORKSPACE before launching anything.  Runs on the current
- * device; the first call on a device looks up the array's device address
- * (cudaGetSymbolAddress), so make it before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race and must be serialised.
- * FP64 path only; device-side errors are reported in point_status. */
+ * device; the first call on a device (and in a new context, e.g. after
+ * cudaDeviceReset) looks up the array's device address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  With CUDA's
+ * lazy module loading (the default) that first call is also when the array
+ * is allocated: make it before the caller's memory pool reserves the device,
+ * or set CUDA_MODULE_LOADING=EAGER.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised.  FP64 path only.
+ * point_status ([P] int32) is required: every device-side error -- the
+ * observation errors of sbletkf_prepare_obs (SBLETKF_ERR_OBS_CELL,
+ * SBLETKF_ERR_NONFINITE), which belong to no point, OR-ed into every entry,
+ * and each point's own analysis errors -- is reported there. */
 #define SBLETKF_NOALLOC_MAX_OBS   8192
 #define SBLETKF_NOALLOC_MAX_CELLS 65536
 int sbletkf_analysis_noalloc(const sbletkf_params *p, const sbletkf_grid *grid, const sbletkf_obs *obs,

@@ -28,7 +28,8 @@ _NAMES = {ERR_ARG: "bad argument", ERR_CUDA: "CUDA error", ERR_WORKSPACE: "works
 EXPORTS = ("sbletkf_abi_version", "sbletkf_workspace_create", "sbletkf_workspace_destroy",
            "sbletkf_prepare_obs", "sbletkf_analysis", "sbletkf_count_nobsl", "sbletkf_get_status",
            "sbletkf_core_batched", "sbletkf_backward", "sbletkf_analysis_noalloc",
-           "sbletkf_obs_operator", "sbletkf_ensemble_mean_spread", "sbletkf_workspace_set_schedule")
+           "sbletkf_obs_operator", "sbletkf_ensemble_mean_spread", "sbletkf_workspace_set_schedule",
+           "sbletkf_latch_status")
 NOALLOC_MAX_OBS, NOALLOC_MAX_CELLS = 8192, 65536
 
 
@@ -89,6 +90,7 @@ def load(path: str = LIB_PATH):
                                   ctypes.POINTER(CObsOut), vp, vp], ctypes.c_int),
         "sbletkf_ensemble_mean_spread": ([pp, i32, vp, vp, i32, vp, vp, vp, vp, vp], ctypes.c_int),
         "sbletkf_workspace_set_schedule": ([vp, i32], ctypes.c_int),
+        "sbletkf_latch_status": ([vp, i32, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

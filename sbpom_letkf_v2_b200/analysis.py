@@ -209,6 +209,11 @@ class Analysis:
         _abi.check(self.lib.sbletkf_get_status(self._ws, _stream_ptr(stream), ctypes.byref(st)), "get_status")
         return int(st.value)
 
+    def latch_status(self, bits: int, stream=None) -> None:
+        """OR `bits` into the latched device status (failure injection on the
+        host, for tests of the error paths)."""
+        _abi.check(self.lib.sbletkf_latch_status(self._ws, int(bits), _stream_ptr(stream)), "latch_status")
+
     def raise_status(self, stream=None) -> None:
         st = self.status(stream)
         if st:

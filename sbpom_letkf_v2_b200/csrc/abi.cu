@@ -37,6 +37,9 @@ static bool grid_ok(const sbletkf_grid *g) {
          g->depth1;
 }
 
+// status |= bits (sbletkf_latch_status)
+__global__ void k_latch(int32_t *status, int32_t bits) { atomicOr(status, bits); }
+
 static bool same_shape(const sbletkf_workspace *ws, const sbletkf_params *p) {
   return ws->p.nmem == p->nmem && ws->p.nlon == p->nlon && ws->p.nlat == p->nlat && ws->p.nlev == p->nlev;
 }
@@ -196,6 +199,13 @@ int sbletkf_get_status(sbletkf_workspace *ws, void *stream, int32_t *status) {
   return SBLETKF_OK;
 }
 
+int sbletkf_latch_status(sbletkf_workspace *ws, int32_t bits, void *stream) {
+  if (!ws) return SBLETKF_ERR_ARG;
+  if (cudaSetDevice(ws->device) != cudaSuccess) return SBLETKF_ERR_CUDA;
+  k_latch<<<1, 1, 0, (cudaStream_t)stream>>>(ws->d_status, bits);
+  return cuda_status(cudaGetLastError());
+}
+
 int sbletkf_core_batched(const sbletkf_params *p, int32_t npts, const int64_t *off, const double *hdxf,
                          const double *rdiag, const double *rloc, const double *dep, double *wvec, double *wmat,
                          const double *uniforms, int32_t *resample_src, int32_t *point_status, void *stream) {
@@ -203,7 +213,6 @@ int sbletkf_core_batched(const sbletkf_params *p, int32_t npts, const int64_t *o
   if (st) return st;
   if (npts < 0 || (npts > 0 && (!off || !wvec || !wmat))) return SBLETKF_ERR_ARG;
   if (p->iswitch_da != SBLETKF_DA_LETKF && npts > 0 && !uniforms) return SBLETKF_ERR_ARG;
-  if (p->precision == SBLETKF_PREC_MIXED) return SBLETKF_ERR_UNSUPPORTED;
   int *d_status = nullptr;
   if (cudaGetSymbolAddress((void **)&d_status, g_core_status) != cudaSuccess) return SBLETKF_ERR_CUDA;
   return launch_core_batched(p, npts, off, hdxf, rdiag, rloc, dep, wvec, wmat, uniforms, resample_src,

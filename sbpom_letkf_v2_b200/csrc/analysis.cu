@@ -18,192 +18,10 @@
 //   W    = sqrt(k-1) [ alpha^-1/2 I + Z^T Q diag(g) Q^T Z ],
 //   g_j  = -1 / ( sqrt(alpha lambda_j) (sqrt(lambda_j) + sqrt(alpha)) ),
 // exact algebra (push-through identity), so only an n x n eigensolve is needed.
-#include "point.cuh"
+#include "tc_point.cuh"
 
 namespace sbl {
 namespace {
-
-// State of the tensor-core Gram pipeline of one CTA (uniform across threads).
-struct TcState {
-  uint32_t tbase;   // TMEM base: sum hi, sum lo, chunk accumulators 0 and 1 (KP columns each)
-  int uses[2];      // commits issued per operand stage
-  int nchunk;
-  int nflushed;     // chunk pairs added into the running sum
-  int broken;       // a wait timed out: issue nothing more
-};
-
-// Add chunk accumulator a (0, 1) into the running double-FP32 sum with
-// Knuth's TwoSum (hi + c = s_ + e exactly; lo += e).  Whole CTA: warp w owns
-// TMEM lanes 32 (w % 4) .. +31 and half w / 4 of the 16-column groups.
-template <int KP>
-__device__ __forceinline__ void tc_flush(TcState &st, int s) {
-  using namespace tc;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  (void)lane;
-  const int q = wid & 3, half = wid >> 2;
-  const uint32_t trow = st.tbase + ((uint32_t)(32 * q) << 16);
-  const uint32_t cc = (uint32_t)((2 + s) * KP);
-  const bool first = st.nflushed == 0;
-  float c[16], h[16], l[16];
-  for (int ch = half; ch < KP / 16; ch += 2) {
-    tmem_ld16(trow + cc + 16 * ch, c);
-    if (first) {
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        h[i] = c[i];
-        l[i] = 0.0f;
-      }
-    } else {
-      tmem_ld16(trow + 16 * ch, h);
-      tmem_ld16(trow + KP + 16 * ch, l);
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const float t = __fadd_rn(h[i], c[i]);
-        const float bv = __fsub_rn(t, h[i]);
-        const float e = __fadd_rn(__fsub_rn(h[i], __fsub_rn(t, bv)), __fsub_rn(c[i], bv));
-        h[i] = t;
-        l[i] = __fadd_rn(l[i], e);
-      }
-    }
-    tmem_st16(trow + 16 * ch, h);
-    tmem_st16(trow + KP + 16 * ch, l);
-  }
-  tmem_wait_st();
-  st.nflushed++;
-}
-
-// Stage `cnt` list entries starting at f as BF16 h/m/l operand tiles and issue
-// their six UMMAs per K-block.  Chunks 2p and 2p+1 share chunk accumulator
-// p % 2 (FP32 over 128 observations); at chunk 2p+3, whose entry wait on
-// stage 1 covers chunk 2p+1's UMMAs, pair p is added into the running sum,
-// before chunk 2p+4 starts that accumulator afresh.  Also
-// accumulates b = sum w dep y (FP64) and, when do_pf, the PF log-likelihood.
-// Whole CTA; ends with the tiles handed to the tensor core.
-template <int KP>
-__device__ __forceinline__ void tc_chunk(const PointSmem &S, const ObsView &ob, TcState &st, uint64_t *mbar,
-                                         int f, int cnt, int k, bool do_pf, double &bacc, double &llacc,
-                                         int &bits) {
-  using namespace tc;
-  const int tid = threadIdx.x;
-  const int s = st.nchunk & 1;
-  float *stg = reinterpret_cast<float *>(S.u);  // [kKC][KP] FP32 rows
-  unsigned char *tiles = reinterpret_cast<unsigned char *>(S.u) + PointSmem::tc_tiles_off(KP);
-  unsigned char *stage = tiles + s * kStageBytes;
-  float *sw = reinterpret_cast<float *>(S.cw);
-  __shared__ int s_broken;
-  if (tid == 0) {  // the stage's previous UMMAs must be done
-    if (!st.broken && st.uses[s] > 0 && !mbar_wait(&mbar[s], (uint32_t)((st.uses[s] - 1) & 1))) {
-      bits |= SBLETKF_ERR_TIMEOUT;
-      s_broken = 1;
-    } else {
-      s_broken = st.broken;
-    }
-  }
-  constexpr int KP4 = KP / 4;
-  for (int e = tid; e < kKC * KP4; e += kThreads) {
-    const int cc = e / KP4, col = e - cc * KP4;
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (cc < cnt) v = reinterpret_cast<const float4 *>(ob.hdxf32 + (long)S.lidx[f + cc] * ob.ldh)[col];
-    reinterpret_cast<float4 *>(stg)[e] = v;
-  }
-  if (tid < kKC) sw[tid] = tid < cnt ? (float)sqrt(S.lw[f + tid]) : 0.0f;
-  __syncthreads();
-  st.broken = s_broken;
-  if (!st.broken && (st.nchunk & 1) && st.nchunk >= 3) {  // pair (nchunk - 3) / 2 is complete: add it
-    fence_after_sync();
-    tc_flush<KP>(st, ((st.nchunk >> 1) + 1) & 1);
-    fence_before_sync();
-  }
-  if (tid < KP)
-    for (int cc = 0; cc < cnt; ++cc) bacc = fma(S.lwd[f + cc], (double)stg[cc * KP + tid], bacc);
-  if (do_pf && tid < k) {
-    for (int cc = 0; cc < cnt; ++cc) {
-      double d = __dsub_rn(S.ldep[f + cc], (double)stg[cc * KP + tid]);
-      double q = __dmul_rn(__dmul_rn(0.5, d), d);
-      q = __ddiv_rn(__dmul_rn(q, S.lrloc[f + cc]), S.lrdiag[f + cc]);
-      llacc = __dsub_rn(llacc, q);
-    }
-  }
-  for (int e = tid; e < kM * (kKC / 8); e += kThreads) {
-    const int m = e & (kM - 1), g = e >> 7;
-    float z[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int o = g * 8 + i;
-      z[i] = m < KP ? sw[o] * stg[o * KP + m] : 0.0f;
-    }
-    store_split8(stage, tile_off(m, g * 8), z);
-  }
-  fence_async_smem();
-  __syncthreads();
-  if (tid == 0 && !st.broken) {
-    fence_after_sync();
-    const uint32_t idesc = idesc_bf16(kM, KP);
-    const uint32_t a0 = smem_u32(stage);
-#pragma unroll
-    for (int kb = 0; kb < kKC / kKB; ++kb) {
-      const uint64_t dh = sdesc(a0 + kb * kBlockBytes), dm = sdesc(a0 + kTileBytes + kb * kBlockBytes),
-                     dl = sdesc(a0 + 2 * kTileBytes + kb * kBlockBytes);
-      const uint32_t acc = (kb > 0 || (st.nchunk & 1)) ? 1u : 0u;  // each pair starts a fresh accumulator
-      const uint32_t d = st.tbase + (uint32_t)((2 + ((st.nchunk >> 1) & 1)) * KP);
-      mma_bf16(d, dh, dh, idesc, acc);  // H^T H
-      mma_bf16(d, dh, dm, idesc, 1u);   // H^T M
-      mma_bf16(d, dm, dh, idesc, 1u);   // M^T H
-      mma_bf16(d, dh, dl, idesc, 1u);   // H^T L
-      mma_bf16(d, dl, dh, idesc, 1u);   // L^T H
-      mma_bf16(d, dm, dm, idesc, 1u);   // M^T M
-    }
-    commit_to(&mbar[s]);
-  }
-  st.uses[s]++;
-  st.nchunk++;
-}
-
-// Wait for every issued UMMA, add the pairs not yet flushed (at most two) into
-// the running sum, then
-// G + alpha I = hi + lo + alpha I into B (FP64, column-major, stride ldb; the
-// lower triangle read and mirrored, so B is exactly symmetric) and b into S.b.
-template <int KP>
-__device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint64_t *mbar, int k, double alpha,
-                                          double bacc, int &bits) {
-  using namespace tc;
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  __shared__ int s_brk;
-  if (tid == 0) {
-    int brk = st.broken;
-    for (int s = 0; s < 2; ++s)
-      if (!brk && st.uses[s] > 0 && !mbar_wait(&mbar[s], (uint32_t)((st.uses[s] - 1) & 1))) {
-        bits |= SBLETKF_ERR_TIMEOUT;
-        brk = 1;
-      }
-    s_brk = brk;
-  }
-  __syncthreads();
-  st.broken = s_brk;
-  fence_after_sync();
-  if (!st.broken)
-    for (int pr = st.nflushed; pr <= ((st.nchunk - 1) >> 1); ++pr) tc_flush<KP>(st, pr & 1);
-  double *B = S.u;
-  const int q = wid & 3, half = wid >> 2, r = 32 * q + lane;
-  const uint32_t trow = st.tbase + ((uint32_t)(32 * q) << 16);
-  float vh[16], vl[16];
-  for (int ch = half; ch < KP / 16; ch += 2) {  // row r, columns c <= r
-    tmem_ld16(trow + 16 * ch, vh);
-    tmem_ld16(trow + KP + 16 * ch, vl);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int c = 16 * ch + i;
-      if (r < k && c <= r) {
-        const double g = (double)vh[i] + (double)vl[i] + (r == c ? alpha : 0.0);
-        B[(long)c * S.ldb + r] = g;
-        B[(long)r * S.ldb + c] = g;
-      }
-    }
-  }
-  if (tid < k) S.b[tid] = bacc;
-  fence_before_sync();
-  __syncthreads();
-}
 
 // Analysis of grid point pid by the whole CTA (the body of the (k,i) loop of
 // da_main).  With vprev != nullptr (persistent, column-ordered launch) a
@@ -303,6 +121,16 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
   // the list is kept for the observation-space transform.
   Accum<R> A;
   A.zero();
+  // tensor-core staging: FP32 rows of the sorted observations, by list index
+  const auto rows = [&](float *stg, int f, int cnt) {
+    constexpr int KP4 = KP / 4;
+    for (int e = tid; e < tc::kKC * KP4; e += kThreads) {
+      const int cc = e / KP4, col = e - cc * KP4;
+      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (cc < cnt) v = reinterpret_cast<const float4 *>(ob.hdxf32 + (long)S.lidx[f + cc] * ob.ldh)[col];
+      reinterpret_cast<float4 *>(stg)[e] = v;
+    }
+  };
   int L = 0, nacc = 0;
   const int ndm = do_gram ? PointSmem::dual_max(k) : -1;
   bool primal = ndm < 0;
@@ -348,7 +176,7 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
     int f = 0;
     if (use_tc) {
       while (L - f >= tc::kKC) {
-        tc_chunk<KP>(S, ob, tcs, s_mbar, f, tc::kKC, k, do_pf, A.b, A.ll, bits);
+        tc_chunk<KP>(S, rows, tcs, s_mbar, f, tc::kKC, k, do_pf, A.b, A.ll, bits);
         f += tc::kKC;
       }
     }
@@ -378,7 +206,7 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
     }
     L = rem;
   }
-  if (use_tc && primal && L > 0) tc_chunk<KP>(S, ob, tcs, s_mbar, 0, L, k, do_pf, A.b, A.ll, bits);
+  if (use_tc && primal && L > 0) tc_chunk<KP>(S, rows, tcs, s_mbar, 0, L, k, do_pf, A.b, A.ll, bits);
   if (!use_tc && primal && L > 0) {
     constexpr int KP2 = KP / 2;
     for (int e = tid; e < L * KP2; e += kThreads) {
@@ -651,32 +479,27 @@ __global__ void __launch_bounds__(kThreads, 1)
   const bool do_gram = p.iswitch_da != SBLETKF_DA_LPF;
   __shared__ uint64_t s_mbar[2];
   __shared__ uint32_t s_tmem;
-  constexpr uint32_t kTmemCols = (4 * KP <= 128) ? 128 : (4 * KP <= 256) ? 256 : 512;
   const bool tc_on = MIXED && do_gram;  // TMEM and barriers held by this CTA
   TcState tcs;
   tcs.uses[0] = tcs.uses[1] = 0;
+  tcs.issued[0] = tcs.issued[1] = 0;
   tcs.nchunk = 0;
   tcs.nflushed = 0;
   tcs.tbase = 0;
   tcs.broken = 0;
-  if (tc_on) {
-    __shared__ int s_abort;
-    if (tid == 0) s_abort = (*(volatile int *)status & SBLETKF_ERR_TIMEOUT) != 0;
-    __syncthreads();
-    if (s_abort) {
-      if (tid == 0 && pst && !queue) pst[p0 + blockIdx.x] = SBLETKF_ERR_TIMEOUT;
-      return;
-    }
-    if ((tid >> 5) == 0) tc::tmem_alloc(&s_tmem, kTmemCols);
-    if (tid == 0) {
-      tc::mbar_init(&s_mbar[0], 1);
-      tc::mbar_init(&s_mbar[1], 1);
-    }
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    tcs.tbase = s_tmem;
+  // A launch that finds SBLETKF_ERR_TIMEOUT already latched (a tensor-core
+  // wait expired earlier) allocates no tensor memory and issues no UMMA: one
+  // CTA per point marks its point and returns; the persistent launch still
+  // drains its queue, and analyze_point marks every point it takes.
+  __shared__ int s_abort;
+  if (tid == 0) s_abort = tc_on && (*(volatile int *)status & SBLETKF_ERR_TIMEOUT) != 0;
+  __syncthreads();
+  const bool aborted = s_abort != 0;
+  if (aborted && !queue) {
+    if (tid == 0 && pst) pst[p0 + blockIdx.x] = SBLETKF_ERR_TIMEOUT;
+    return;
   }
+  if (tc_on && !aborted) tc_open<KP>(tcs, s_mbar, &s_tmem);
   // one call site of the point body for both schedules.  Column schedule: a
   // queue item is up to colchunk (1..8) columns cstride apart -- with cstride
   // = nlon, neighbours along a meridian -- walked in snake order (levels down,
@@ -719,14 +542,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     analyze_point<R, ST, MIXED>(p, g, ob, f3, f2, a3, a2, uni, src_out, pst, status, S, tcs, s_mbar, tc_on, pid,
                                 vprev, xtmp, warm);
   }
-  if (tc_on) {  // every UMMA was waited for in tc_finish (or never issued)
-    tc::fence_before_sync();
-    __syncthreads();
-    if ((tid >> 5) == 0) {
-      tc::fence_after_sync();
-      tc::tmem_dealloc(tcs.tbase, kTmemCols);
-    }
-  }
+  if (tc_on && !aborted) tc_close<KP>(tcs, s_mbar, status);
 }
 
 // count_nobsl (common_da.f90:133-205): one warp per point.

@@ -7,12 +7,15 @@
 //   lpfgm_core_noobs  letkf/run/src/common_lpfgm.f90:422-440
 // Point q's inputs are the Fortran arrays hdxf(nobsl,nmem), rdiag, rloc, dep
 // starting at row off[q].  W is written column-major, W(i,j) at j*k+i.
-#include "point.cuh"
+// With SBLETKF_PREC_MIXED the Gram runs on the tensor cores exactly as in the
+// analysis kernel (tc_point.cuh, FP32 rows of hdxf), so W states the mixed
+// path's error against letkf_core.
+#include "tc_point.cuh"
 
 namespace sbl {
 namespace {
 
-template <int R>
+template <int R, bool MIXED>
 __global__ void __launch_bounds__(kThreads, 1)
     k_core(const sbletkf_params p, const int64_t *__restrict__ off, const double *__restrict__ hdxf,
            const double *__restrict__ rdiag, const double *__restrict__ rloc, const double *__restrict__ dep,
@@ -36,8 +39,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   Accum<R> A;
   A.zero();
-  for (int f = 0; f < n; f += kChunk) {
-    const int cnt = min(kChunk, n - f);
+  const auto fill_list = [&](int f, int cnt) {
     if (tid < cnt) {
       const long long r = o0 + f + tid;
       const double rl = rloc[r], rd = rdiag[r], dp = dep[r];
@@ -47,12 +49,37 @@ __global__ void __launch_bounds__(kThreads, 1)
       S.lw[tid] = rl / rd;
       S.lwd[tid] = (rl / rd) * dp;
     }
-    for (int e = tid; e < cnt * KP; e += kThreads) {
-      const int m = e / cnt, cc = e - m * cnt;
-      S.u[cc * KP + m] = m < k ? hq[(long long)m * n + f + cc] : 0.0;
+  };
+  __shared__ uint64_t s_mbar[2];
+  __shared__ uint32_t s_tmem;
+  TcState tcs;
+  const bool tc_on = MIXED && do_gram;
+  if (tc_on) {
+    tc_open<KP>(tcs, s_mbar, &s_tmem);
+    // FP32 rows of the chunk: stg[cc][m] = hdxf(f+cc, m) (Fortran order in hq)
+    const auto rows = [&](float *stg, int f, int cnt) {
+      for (int e = tid; e < tc::kKC * KP; e += kThreads) {
+        const int m = e / tc::kKC, cc = e - m * tc::kKC;
+        stg[cc * KP + m] = (m < k && cc < cnt) ? (float)hq[(long long)m * n + f + cc] : 0.0f;
+      }
+    };
+    for (int f = 0; f < n; f += tc::kKC) {
+      const int cnt = min(tc::kKC, n - f);
+      fill_list(f, cnt);
+      __syncthreads();
+      tc_chunk<KP>(S, rows, tcs, s_mbar, 0, cnt, k, do_pf, A.b, A.ll, bits);
     }
-    __syncthreads();
-    accumulate_chunk<R>(S, 0, cnt, k, do_gram, do_pf, A);
+  } else {
+    for (int f = 0; f < n; f += kChunk) {
+      const int cnt = min(kChunk, n - f);
+      fill_list(f, cnt);
+      for (int e = tid; e < cnt * KP; e += kThreads) {
+        const int m = e / cnt, cc = e - m * cnt;
+        S.u[cc * KP + m] = m < k ? hq[(long long)m * n + f + cc] : 0.0;
+      }
+      __syncthreads();
+      accumulate_chunk<R>(S, 0, cnt, k, do_gram, do_pf, A);
+    }
   }
 
   if (n == 0) {
@@ -62,7 +89,8 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else {
     if (do_gram) {
       const double alpha = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
-      store_gram<R>(S, k, alpha, A);
+      if (tc_on) tc_finish<KP>(S, tcs, s_mbar, k, alpha, A.b, bits);
+      else store_gram<R>(S, k, alpha, A);
       const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
       bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
       vt_times(S.u, k, S.ldb, S.b, S.c);
@@ -150,9 +178,15 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int e = tid; e < k; e += kThreads) wv[e] = 0.0;
     }
   }
+  if (tc_on) tc_close<KP>(tcs, s_mbar, status);
+  __shared__ int s_bits;
+  if (tid == 0) s_bits = 0;
+  __syncthreads();
+  if (bits) atomicOr(&s_bits, bits);
+  __syncthreads();
   if (tid == 0) {
-    if (pst) pst[q] = bits;
-    if (bits) atomicOr(status, bits);
+    if (pst) pst[q] = s_bits;
+    if (s_bits) atomicOr(status, s_bits);
   }
 }
 
@@ -160,8 +194,9 @@ template <int R>
 int launch_core_r(const sbletkf_params *p, int32_t npts, const int64_t *off, const double *hdxf,
                   const double *rdiag, const double *rloc, const double *dep, double *wvec, double *wmat,
                   const double *uni, int32_t *src, int32_t *pst, int *d_status, cudaStream_t s) {
-  const size_t smem = PointSmem::bytes(p->nmem, kp_of_r(R));
-  auto kern = k_core<R>;
+  const bool mixed = p->precision == SBLETKF_PREC_MIXED;
+  const size_t smem = PointSmem::bytes(p->nmem, kp_of_r(R), mixed);
+  auto kern = mixed ? k_core<R, true> : k_core<R, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_status(e);
   kern<<<npts, kThreads, smem, s>>>(*p, off, hdxf, rdiag, rloc, dep, wvec, wmat, uni, src, pst, d_status);

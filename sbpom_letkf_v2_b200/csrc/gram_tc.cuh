@@ -38,6 +38,7 @@ constexpr int kTileBytes = kBlockBytes * (kKC / kKB);  // one chunk of one split
 constexpr int kSplit = 3;                              // h, m, l
 constexpr int kStageBytes = kSplit * kTileBytes;
 constexpr unsigned kWaitLimit = 1u << 20;              // bounded mbarrier polls
+constexpr unsigned kDrainLimit = 1u << 26;             // polls of the drain before TMEM is freed
 // Largest search-box candidate count whose Gram goes to the tensor cores: the
 // FP32 accumulator's rounding grows like eps32 sqrt(n/16) |G|, which must stay
 // well below alpha = (k-1)/rho for the eigensolve; denser points use FP64.
@@ -93,10 +94,10 @@ __device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
 }
 
-// Wait for phase `parity` of an mbarrier; false after kWaitLimit polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+// Wait for phase `parity` of an mbarrier; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity, unsigned limit = kWaitLimit) {
   const uint32_t a = smem_u32(mbar);
-  for (unsigned it = 0; it < kWaitLimit; ++it) {
+  for (unsigned it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"

@@ -77,3 +77,28 @@ def test_point_status_marks_the_failing_points(cuda):
     assert code & ERR_EIG_NOCONV and bool(bad.any())
     assert bool((nobsl[bad] > 0).all())   # only points with observations run the eigensolve
     an.close()
+
+
+@pytest.mark.parametrize("schedule", [Analysis.SCHED_COLUMNS, Analysis.SCHED_POINT])
+def test_prelatched_timeout_aborts_mixed_launch_and_context_stays_usable(schedule, cuda):
+    """The path every tensor-core launch takes once a bounded wait has expired
+    somewhere: with SBLETKF_ERR_TIMEOUT latched on the host before the launch,
+    no CTA allocates tensor memory or issues a UMMA, every point is marked,
+    the call reports the status, and the next call runs normally."""
+    from sbpom_letkf_v2_b200._abi import ERR_TIMEOUT
+    case = _case()
+    p = case.params.replace(precision=1)
+    P = p.nlev * case.nij1
+    an = Analysis(p, case.nij1, case.obs["elm"].numel(), device="cuda:0")
+    an.set_schedule(schedule)
+    an.prepare_obs(case.obs)
+    st = torch.zeros(P, dtype=torch.int32, device="cuda:0")
+    an.latch_status(ERR_TIMEOUT)
+    an.da_main(case.grid, case.fcst3d, case.fcst2d, point_status=st, check=False)
+    assert an.status() & ERR_TIMEOUT
+    assert bool(((st & ERR_TIMEOUT) != 0).all())
+    st.zero_()
+    a3, a2 = an.da_main(case.grid, case.fcst3d, case.fcst2d, point_status=st)   # raises on any status
+    assert torch.isfinite(a3).all() and torch.isfinite(a2).all()
+    assert bool((st == 0).all())
+    an.close()
