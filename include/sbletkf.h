@@ -103,7 +103,11 @@ typedef struct sbletkf_params {
   double jacobi_tol;   /* relative off-diagonal tolerance of the eigensolve   */
   double tc_max_cand;  /* mixed path: points whose search box holds more candidates
                           use the FP64 Gram; <= 0: library default 12288   */
-  double reserved_d[2];
+  double jacobi_stop;  /* the eigensolve ends after a sweep whose largest relative
+                          rotation |b_p.b_q| / (|b_p||b_q|) was at most this
+                          (convergence is quadratic: what remains is ~its
+                          square); <= 0: library default 1e-7              */
+  double reserved_d[1];
 } sbletkf_params;
 
 /* Local grid of the points analysed (set_common_mpi_pom, common_pom.f90:125-219) */

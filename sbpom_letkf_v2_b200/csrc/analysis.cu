@@ -262,7 +262,7 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
     }
     __syncthreads();
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
-    bits |= jacobi_eig<(KP / 4 < 16 ? KP / 4 : 16)>(Nb, n, ldn, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+    bits |= jacobi_eig<(KP / 4 < 16 ? KP / 4 : 16)>(Nb, n, ldn, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
     vt_times(Nb, n, ldn, S.b, S.c);  // c = Lambda^-1 Q^T d
     __syncthreads();
     if (tid < n) S.c[tid] /= S.lam[tid];
@@ -273,9 +273,9 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
     else store_gram<R>(S, k, alpha, A);
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
     if (vprev && warm)  // start from the previous level's eigenvectors
-      bits |= jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.cw, vprev, xtmp);
+      bits |= jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.cw, vprev, xtmp);
     else
-      bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+      bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
     if (vprev) {  // keep this level's eigenvectors for the next one
       for (int e = tid; e < k * k; e += kThreads) vprev[e] = S.u[(long)(e / k) * S.ldb + (e % k)];
       warm = 1;

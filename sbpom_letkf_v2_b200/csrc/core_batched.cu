@@ -56,16 +56,18 @@ __global__ void __launch_bounds__(kThreads, 1)
   const bool tc_on = MIXED && do_gram;
   if (tc_on) {
     tc_open<KP>(tcs, s_mbar, &s_tmem);
-    // FP32 rows of the chunk: stg[cc][m] = hdxf(f+cc, m) (Fortran order in hq)
-    const auto rows = [&](float *stg, int f, int cnt) {
+    // FP32 rows of the chunk at observation f0: stg[cc][m] = hdxf(f0+cc, m)
+    // (Fortran order in hq); the chunk's list entries sit at [0, cnt)
+    int f0 = 0;
+    const auto rows = [&](float *stg, int, int cnt) {
       for (int e = tid; e < tc::kKC * KP; e += kThreads) {
         const int m = e / tc::kKC, cc = e - m * tc::kKC;
-        stg[cc * KP + m] = (m < k && cc < cnt) ? (float)hq[(long long)m * n + f + cc] : 0.0f;
+        stg[cc * KP + m] = (m < k && cc < cnt) ? (float)hq[(long long)m * n + f0 + cc] : 0.0f;
       }
     };
-    for (int f = 0; f < n; f += tc::kKC) {
-      const int cnt = min(tc::kKC, n - f);
-      fill_list(f, cnt);
+    for (; f0 < n; f0 += tc::kKC) {
+      const int cnt = min(tc::kKC, n - f0);
+      fill_list(f0, cnt);
       __syncthreads();
       tc_chunk<KP>(S, rows, tcs, s_mbar, 0, cnt, k, do_pf, A.b, A.ll, bits);
     }
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       if (tc_on) tc_finish<KP>(S, tcs, s_mbar, k, alpha, A.b, bits);
       else store_gram<R>(S, k, alpha, A);
       const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
-      bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+      bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
       vt_times(S.u, k, S.ldb, S.b, S.c);
       __syncthreads();
       if (tid < k) S.c[tid] /= S.lam[tid];

@@ -20,6 +20,13 @@
 
 namespace sbl {
 
+// Relative rotation size that ends the Jacobi eigensolve (see
+// jacobi_sweeps_oe) unless sbletkf_params.jacobi_stop sets another.
+constexpr double kJacobiStop = 1e-7;
+__host__ __device__ inline double jacobi_stop_of(const sbletkf_params &p) {
+  return p.jacobi_stop > 0.0 ? p.jacobi_stop : kJacobiStop;
+}
+
 // R x R register tile per thread over a 16 x 16 thread grid: k <= 16*R.
 __host__ __device__ constexpr int kp_of_r(int r) { return 16 * r; }
 inline int r_for_k(int k) { return k <= 32 ? 2 : k <= 64 ? 4 : k <= 112 ? 7 : 8; }
@@ -213,9 +220,11 @@ __device__ __forceinline__ void store_gram(const PointSmem &S, int k, double alp
 // rotated when (b_p.b_q)^2 > tol^2 |b_p|^2 |b_q|^2; the angle t is computed
 // in FP32 while c = 1/sqrt(1+t^2), s = c t are FP64, so every rotation is
 // orthogonal to FP64 rounding and the angle only has to shrink b_p.b_q (the
-// residual of a rotation is ~1e-7 of what it removes).  A sweep whose largest
-// relative b_p.b_q was below 1e-10 leaves the columns orthogonal to working
-// precision, so the loop ends after it.
+// residual of a rotation is ~1e-7 of what it removes).  Convergence is
+// quadratic: after a sweep whose largest relative b_p.b_q was g the next
+// sweep's are ~g^2, so the loop ends after a sweep with g <= `stop` (1e-7 by
+// default, leaving ~1e-14, far below the parity tolerance) instead of running
+// one more sweep only to confirm it.
 // ---------------------------------------------------------------------------
 
 // In-place pivoted Cholesky of the full symmetric matrix in B: on return B's
@@ -311,8 +320,8 @@ static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *pe
 // padding column of odd n is dropped), which is all the eigenpair extraction
 // needs.  nrm: >= n doubles of scratch; flag: >= 4 shared ints.
 template <int E>
-static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb, double tol, int maxsw, double *nrm,
-                                                       int *flag) {
+static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb, double tol, double stop, int maxsw,
+                                                       double *nrm, int *flag) {
   constexpr int G = 4;
   const int tid = threadIdx.x, gl = tid % G, grp = tid / G, lane = tid & 31;
   const int n2 = (n + 1) & ~1, ng = n2 / 2;   // 2*ng - 1 <= n slots fit in B
@@ -329,7 +338,7 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
     }
   }
   __syncthreads();
-  const double tol2 = tol * tol, big2 = 1e-20;
+  const double tol2 = tol * tol, big2 = stop * stop;
   int sweep = 0;
   for (; sweep < maxsw; ++sweep) {
     {  // exact squared norms at the start of a sweep
@@ -468,15 +477,15 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
 // lam[] receives the eigenvalues.  vec: n doubles, perm: n ints of scratch;
 // flag: >= 4 shared ints (flag[3] = sweeps run).  Returns status bits.
 template <int EMAX>
-static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, double tol, int maxsw, double *lam,
-                                                 int *flag, int *perm, double *vec) {
+static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, double tol, double stop, int maxsw,
+                                                 double *lam, int *flag, int *perm, double *vec) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   int bits = chol_pivot(B, n, ldb, perm, vec, flag);
-  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps_oe<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps_oe<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, maxsw, vec, flag);
-  else bits |= jacobi_sweeps_oe<EMAX>(B, n, ldb, tol, maxsw, vec, flag);
+  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, stop, maxsw, vec, flag);
+  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, stop, maxsw, vec, flag);
+  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps_oe<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, stop, maxsw, vec, flag);
+  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps_oe<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, stop, maxsw, vec, flag);
+  else bits |= jacobi_sweeps_oe<EMAX>(B, n, ldb, tol, stop, maxsw, vec, flag);
   // lambda_j = |column j|^2; eigenvector = column / |column|, rows un-permuted
   for (int j = wid; j < n; j += nw) {
     double *cj = B + (long)j * ldb;
@@ -514,8 +523,8 @@ static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, doub
 // matrix V came from, X starts nearly orthogonal and needs a few sweeps
 // instead of the cold solve's pivoted Cholesky and ~10 sweeps.
 template <int EMAX>
-static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb, double tol, int maxsw, double *lam,
-                                                      int *flag, double *vec, const double *V, double *X) {
+static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb, double tol, double stop, int maxsw,
+                                                      double *lam, int *flag, double *vec, const double *V, double *X) {
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
   // X = A V, 4 columns of V per thread pass (A symmetric, column q of A = row q)
   for (int e = tid; e < n * ((n + 3) / 4); e += nt) {
@@ -538,11 +547,11 @@ static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb,
   for (int e = tid; e < n * n; e += nt) B[(long)(e / n) * ldb + (e % n)] = X[e];
   __syncthreads();
   int bits = 0;
-  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps_oe<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, maxsw, vec, flag);
-  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps_oe<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, maxsw, vec, flag);
-  else bits |= jacobi_sweeps_oe<EMAX>(B, n, ldb, tol, maxsw, vec, flag);
+  if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, stop, maxsw, vec, flag);
+  else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, stop, maxsw, vec, flag);
+  else if (n <= 100 || EMAX <= 25) bits |= jacobi_sweeps_oe<(EMAX < 25 ? EMAX : 25)>(B, n, ldb, tol, stop, maxsw, vec, flag);
+  else if (n <= 112 || EMAX <= 28) bits |= jacobi_sweeps_oe<(EMAX < 28 ? EMAX : 28)>(B, n, ldb, tol, stop, maxsw, vec, flag);
+  else bits |= jacobi_sweeps_oe<EMAX>(B, n, ldb, tol, stop, maxsw, vec, flag);
   for (int j = wid; j < n; j += nw) {
     double *cj = B + (long)j * ldb;
     double v[4], s = 0.0;

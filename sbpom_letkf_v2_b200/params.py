@@ -44,7 +44,7 @@ class CParams(ctypes.Structure):
         ("smin", ctypes.c_double), ("smax", ctypes.c_double),
         ("re", ctypes.c_double), ("pi", ctypes.c_double),
         ("jacobi_tol", ctypes.c_double), ("tc_max_cand", ctypes.c_double),
-        ("reserved_d", ctypes.c_double * 2),
+        ("jacobi_stop", ctypes.c_double), ("reserved_d", ctypes.c_double * 1),
     ]
 
 
@@ -92,6 +92,7 @@ class LETKFParams:
     pi: float = 4.0 * math.atan(1.0)  # :27
     jacobi_tol: float = 0.0         # 0 -> library default (k * eps)
     tc_max_cand: float = 0.0        # mixed path: FP64 Gram above this many box candidates (0 -> 12288)
+    jacobi_stop: float = 0.0        # end the eigensolve after a sweep with no relative rotation above this (0 -> 1e-7)
 
     def __post_init__(self):
         if self.dist_zero is None:

@@ -135,7 +135,7 @@ def test_noalloc_rejects_sizes_beyond_its_limits(cuda):
     big = {k: (v.repeat(1, reps)[:, :n] if v.dim() == 2 else v.repeat(reps)[:n]) for k, v in big.items()}
     code, _, _, _ = _noalloc(case, cuda, obs=big)
     assert code == _abi.ERR_WORKSPACE
-    wide = WORKLOADS[0].scaled(nlon=300, nlat=220, nlev=1, nmem=8, n_sst=50, n_ssh=0, n_prof=1, seed=508)
+    wide = WORKLOADS[0].scaled(nlon=300, nlat=220, nlev=2, nmem=8, n_sst=50, n_ssh=0, n_prof=1, seed=508)
     assert wide.nlon * wide.nlat > _abi.NOALLOC_MAX_CELLS
     code, _, _, _ = _noalloc(make_case(wide), cuda)
     assert code == _abi.ERR_WORKSPACE
