@@ -43,6 +43,7 @@ TC_MAX_CAND_DEFAULT = 12288.0   # library default of sbletkf_params.tc_max_cand
 # with 2 levels (bench.py --levels 2), which gets the same 8-column queue
 # items, mixed path.  Scaled by the points of a launch.
 DRAM_BYTES_PER_POINT_W1 = 1073.6e6 / 240000.0
+DRAM_SCHEDULE_W1 = "columns"      # the schedule that capture ran
 # The same for the LPF: workload 4 on its 1/2 grid (bench.py --workload 4 --scale 2).
 DRAM_BYTES_PER_POINT_W4 = 280.6e6 / 61440.0
 
@@ -498,8 +499,9 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying CUDA graphs")
     ap.add_argument("--tune", action="store_true",
                     help="pick schedule and tensor-core routing with the autotuner before timing")
-    ap.add_argument("--schedule", choices=["columns", "point"], default="columns",
-                    help="persistent column queue with warm-started eigensolves, or one CTA per point")
+    ap.add_argument("--schedule", choices=["pipeline", "columns", "point"], default="pipeline",
+                    help="pipelined column queue (producer / consumer warps), persistent column queue with "
+                         "warm-started eigensolves, or one CTA per point (the LPF always uses its default)")
     ap.add_argument("--no-aux", action="store_true",
                     help="skip the timing of the observation operator and the ensemble statistics")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -566,7 +568,10 @@ def main():
         uni = uni.reshape(P_local, *uni_full.shape[1:]).contiguous()
 
     an = Analysis(p, ncol, nobs, device=dev)
-    an.set_schedule(Analysis.SCHED_COLUMNS if args.schedule == "columns" else Analysis.SCHED_POINT)
+    sched = {"pipeline": Analysis.SCHED_PIPELINE, "columns": Analysis.SCHED_COLUMNS,
+             "point": Analysis.SCHED_POINT}[args.schedule]
+    if not pf:   # the LPF keeps its default (one CTA per point)
+        an.set_schedule(sched)
     tuned = None
     if args.tune:
         from sbpom_letkf_v2_b200 import tune
@@ -739,7 +744,7 @@ def main():
             tmask = np.broadcast_to((cand <= tmax)[None, :], (p.nlev, ncol)) if prec == PREC_MIXED else None
             fl = algorithmic_flops(nob_l, p.nmem, p.nv3d, p.nv2d, p.nlev, ncol, tmask)
             traffic = (DRAM_BYTES_PER_POINT_W1 * P_local if (args.workload == 1 and prec == PREC_MIXED
-                                                            and args.schedule == "columns") else None)
+                                                            and args.schedule == DRAM_SCHEDULE_W1) else None)
             roof = letkf_roofline(fl, kern_ms, _fp64_peak(dev), peaks, src, traffic)
         cpu = None
         chk = None

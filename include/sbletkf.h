@@ -273,17 +273,24 @@ int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const vo
                                  void *stream);
 
 /* Launch schedule of sbletkf_analysis for this workspace.
- * SBLETKF_SCHED_COLUMNS (the default, except for the LPF): one persistent CTA
- * per SM takes items of up to 8 grid columns, nlon apart (neighbours along a
- * meridian), from an atomic queue and walks their levels in snake order,
- * starting every k x k eigensolve from the eigenvectors of the previous one;
- * items narrow to 1 column when the grid has fewer than 32 items of 8 per CTA.
+ * SBLETKF_SCHED_COLUMNS: one persistent 256-thread CTA per SM takes items of
+ * up to 8 grid columns, nlon apart (neighbours along a meridian), from an
+ * atomic queue and walks their levels in snake order, starting every k x k
+ * eigensolve from the eigenvectors of the previous one; items narrow to 1
+ * column when the grid has fewer than 32 items of 8 per CTA.
+ * SBLETKF_SCHED_PIPELINE (the default for LETKF and LPFGM with nmem <= 112):
+ * the same walk by a warp-specialised 384-thread CTA per SM, whose 4 producer
+ * warps select the local observations of the next point (and, mixed
+ * precision, accumulate its Gram on the tensor cores) while its 8 consumer
+ * warps run the eigensolve and update of the current one.  The workspace
+ * then holds two local-obs lists of max_nobs entries per SM (12 bytes each).
  * SBLETKF_SCHED_POINT (the LPF default, which has no eigensolve): one CTA per
- * grid point.  Both give the same analysis to rounding.
+ * grid point.  All give the same analysis to rounding.
  * No reference counterpart (the reference's OpenMP DYNAMIC loop over (k,i),
  * common_da.f90:66-68, is the scheduling it replaces). */
-#define SBLETKF_SCHED_POINT   0
-#define SBLETKF_SCHED_COLUMNS 1
+#define SBLETKF_SCHED_POINT    0
+#define SBLETKF_SCHED_COLUMNS  1
+#define SBLETKF_SCHED_PIPELINE 2
 int sbletkf_workspace_set_schedule(sbletkf_workspace *ws, int32_t schedule);
 
 /* Vector-Jacobian product of the LETKF analysis (iswitch_da = 1, with RTPP,

@@ -94,7 +94,14 @@ int sbletkf_workspace_create(const sbletkf_params *p, int32_t nij1, int32_t max_
     alloc((void **)&ws->d_queue, sizeof(int32_t) * 4);
     alloc((void **)&ws->d_slab, sizeof(double) * 2 * (size_t)p->nmem * p->nmem * (size_t)(nsm > 0 ? nsm : 1));
     // the LPF has no eigensolve to warm-start: one CTA per point suits it
-    ws->schedule = p->iswitch_da == SBLETKF_DA_LPF ? 0 : 1;
+    ws->schedule = p->iswitch_da == SBLETKF_DA_LPF ? SBLETKF_SCHED_POINT : SBLETKF_SCHED_COLUMNS;
+    if (pipeline_supported(p)) {  // the pipelined schedule's per-CTA local-obs lists
+      ws->list_cap = (long long)no;
+      const size_t nl = (size_t)2 * (size_t)(nsm > 0 ? nsm : 1) * (size_t)ws->list_cap;
+      alloc((void **)&ws->d_list_idx, sizeof(int32_t) * nl);
+      alloc((void **)&ws->d_list_rloc, sizeof(double) * nl);
+      ws->schedule = SBLETKF_SCHED_PIPELINE;
+    }
   }
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ws->h_status, sizeof(int32_t) * 4);
   if (e == cudaSuccess) e = cudaMemset(ws->d_status, 0, sizeof(int32_t) * 4);
@@ -112,7 +119,7 @@ int sbletkf_workspace_destroy(sbletkf_workspace *ws) {
   cudaSetDevice(ws->device);
   void *ptrs[] = {ws->d_elm, ws->d_lon, ws->d_lat, ws->d_lev, ws->d_rdiag, ws->d_dep, ws->d_hdxf64,
                   ws->d_hdxf32, ws->d_perm, ws->d_tmp, ws->d_cellstart, ws->d_cellcnt, ws->d_status,
-                  ws->d_gscratch, ws->d_queue, ws->d_slab};
+                  ws->d_gscratch, ws->d_queue, ws->d_slab, ws->d_list_idx, ws->d_list_rloc};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (ws->h_status) cudaFreeHost(ws->h_status);
@@ -167,7 +174,10 @@ int sbletkf_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const sblet
 }
 
 int sbletkf_workspace_set_schedule(sbletkf_workspace *ws, int32_t schedule) {
-  if (!ws || (schedule != SBLETKF_SCHED_POINT && schedule != SBLETKF_SCHED_COLUMNS)) return SBLETKF_ERR_ARG;
+  if (!ws || (schedule != SBLETKF_SCHED_POINT && schedule != SBLETKF_SCHED_COLUMNS &&
+              schedule != SBLETKF_SCHED_PIPELINE))
+    return SBLETKF_ERR_ARG;
+  if (schedule == SBLETKF_SCHED_PIPELINE && !ws->d_list_idx) return SBLETKF_ERR_UNSUPPORTED;
   ws->schedule = schedule;
   return SBLETKF_OK;
 }

@@ -35,6 +35,12 @@ struct GridView {
 
 __host__ __device__ inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
+// Barrier of the kThreads threads (warps 0..7) that analyse one point.  In
+// the 256-thread kernels that is the whole CTA (the same as __syncthreads);
+// in the warp-specialised analysis kernel it is the consumer warps only, the
+// producer warps synchronise on barrier 2.
+__device__ __forceinline__ void cta_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kThreads) : "memory"); }
+
 // Fortran NINT: nearest integer, halves away from zero (round() semantics).
 __device__ __forceinline__ long long fnint(double x) { return llround(x); }
 
@@ -155,6 +161,11 @@ struct sbletkf_workspace {
   int nslab = 0;
   int32_t *d_queue = nullptr;
   double *d_slab = nullptr;
+  // pipelined schedule: per CTA and slot, the local-obs list of a point
+  // (sorted-obs index and rloc), list_cap entries each
+  int32_t *d_list_idx = nullptr;
+  double *d_list_rloc = nullptr;
+  long long list_cap = 0;
   sbl::ObsView obs_view() const {
     sbl::ObsView v;
     v.nobs = nobs; v.ldh = ldh; v.elm = d_elm; v.lon = d_lon; v.lat = d_lat; v.lev = d_lev;
@@ -176,6 +187,10 @@ int launch_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const GridVi
                     int32_t *pst, cudaStream_t s);
 int launch_count(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, int32_t *nobsl,
                  cudaStream_t s);
+bool pipeline_supported(const sbletkf_params *p);
+int launch_analysis_ws(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, const void *f3,
+                       const void *f2, void *a3, void *a2, int dtype, const double *uni, int32_t *src, int32_t *pst,
+                       cudaStream_t s);
 int launch_core_batched(const sbletkf_params *p, int32_t npts, const int64_t *off, const double *hdxf,
                         const double *rdiag, const double *rloc, const double *dep, double *wvec,
                         double *wmat, const double *uni, int32_t *src, int32_t *pst, int *d_status,

@@ -74,31 +74,35 @@ struct PointSmem {
     m = m > tcb ? m : tcb;
     return a16(m > pf ? m : pf);
   }
-  __host__ __device__ static size_t fixed_bytes(int kp) {
+  // nrows: grid rows of a search box kept (0: none, the rows live
+  // elsewhere); listcap: local-obs list entries (>= dual_max and >= kp,
+  // since the eigensolve borrows lidx as its permutation).
+  __host__ __device__ static size_t fixed_bytes(int kp, int nrows = kRowMax, int listcap = kListCap) {
     size_t s = 0;
-    s += a16(sizeof(int) * kRowMax) + a16(sizeof(int) * (kRowMax + 1)) + a16(sizeof(int) * kListCap) +
-         a16(sizeof(int) * 64);
-    s += 5 * a16(sizeof(double) * kListCap);
+    s += (nrows > 0 ? a16(sizeof(int) * nrows) + a16(sizeof(int) * (nrows + 1)) : 0) +
+         a16(sizeof(int) * listcap) + a16(sizeof(int) * 64);
+    s += 5 * a16(sizeof(double) * listcap);
     s += 5 * a16(sizeof(double) * kp) + a16(sizeof(double) * 64);
     s += 4 * a16(sizeof(double) * kNvMax * kp);
     return s;
   }
-  __host__ __device__ static size_t bytes(int k, int kp, bool mixed = false) {
-    return fixed_bytes(kp) + union_bytes(k, kp, mixed) + (mixed ? 1024 : 0);
+  __host__ __device__ static size_t bytes(int k, int kp, bool mixed = false, int nrows = kRowMax,
+                                          int listcap = kListCap) {
+    return fixed_bytes(kp, nrows, listcap) + union_bytes(k, kp, mixed) + (mixed ? 1024 : 0);
   }
 
-  __device__ void carve(void *base, int k, int kp) {
+  __device__ void carve(void *base, int k, int kp, int nrows = kRowMax, int listcap = kListCap) {
     char *q = (char *)base;
     auto take = [&](size_t n) { char *r = q; q += a16(n); return (void *)r; };
-    rowstart = (int *)take(sizeof(int) * kRowMax);
-    rowpref = (int *)take(sizeof(int) * (kRowMax + 1));
-    lidx = (int *)take(sizeof(int) * kListCap);
+    rowstart = nrows > 0 ? (int *)take(sizeof(int) * nrows) : nullptr;
+    rowpref = nrows > 0 ? (int *)take(sizeof(int) * (nrows + 1)) : nullptr;
+    lidx = (int *)take(sizeof(int) * listcap);
     iws = (int *)take(sizeof(int) * 64);
-    lw = (double *)take(sizeof(double) * kListCap);
-    lwd = (double *)take(sizeof(double) * kListCap);
-    lrloc = (double *)take(sizeof(double) * kListCap);
-    lrdiag = (double *)take(sizeof(double) * kListCap);
-    ldep = (double *)take(sizeof(double) * kListCap);
+    lw = (double *)take(sizeof(double) * listcap);
+    lwd = (double *)take(sizeof(double) * listcap);
+    lrloc = (double *)take(sizeof(double) * listcap);
+    lrdiag = (double *)take(sizeof(double) * listcap);
+    ldep = (double *)take(sizeof(double) * listcap);
     b = (double *)take(sizeof(double) * kp);
     lam = (double *)take(sizeof(double) * kp);
     c = (double *)take(sizeof(double) * kp);
@@ -159,7 +163,7 @@ __device__ __forceinline__ void accumulate_chunk(const PointSmem &S, int f, int 
     // independent: the whole CTA computes them (in place of the rows, which the
     // Gram above has finished with), then each member's thread subtracts its
     // column of terms in observation order -- the same operations and order.
-    if (do_gram) __syncthreads();
+    if (do_gram) cta_sync();
     double *q = S.u;
 #pragma unroll 4
     for (int e = tid; e < cnt * KP; e += kThreads) {
@@ -170,14 +174,14 @@ __device__ __forceinline__ void accumulate_chunk(const PointSmem &S, int f, int 
         q[e] = __ddiv_rn(__dmul_rn(t, S.lrloc[f + cc]), S.lrdiag[f + cc]);
       }
     }
-    __syncthreads();
+    cta_sync();
     if (tid < k) {
       double ll = A.ll;
       for (int cc = 0; cc < cnt; ++cc) ll = __dsub_rn(ll, q[cc * KP + tid]);
       A.ll = ll;
     }
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // Write G + alpha I (k x k, column-major, stride ldb) into B = S.u and b into S.b.
@@ -195,7 +199,7 @@ __device__ __forceinline__ void store_gram(const PointSmem &S, int k, double alp
     }
   if (tid < k) S.b[tid] = A.b;
   (void)KP;
-  __syncthreads();
+  cta_sync();
 }
 
 // ---------------------------------------------------------------------------
@@ -231,11 +235,11 @@ __device__ __forceinline__ void store_gram(const PointSmem &S, int k, double alp
 // lower triangle holds L (P A P^T = L L^T), the strict upper triangle is zero
 // and perm[i] is the original index of row i.  vec: n doubles of scratch.
 static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *perm, double *vec, int *flag) {
-  const int tid = threadIdx.x, nt = blockDim.x, tx = tid & 15, ty = tid >> 4, nty = nt >> 4;
+  const int tid = threadIdx.x, nt = kThreads, tx = tid & 15, ty = tid >> 4, nty = nt >> 4;
   const int lane = tid & 31, wid = tid >> 5;
   for (int i = tid; i < n; i += nt) perm[i] = i;
   if (tid == 0) flag[1] = 0;
-  __syncthreads();
+  cta_sync();
   for (int j = 0; j < n; ++j) {
     if (wid == 0) {  // pivot: largest remaining diagonal (first on ties)
       double best = -1.0;
@@ -258,7 +262,7 @@ static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *pe
       }
       if (lane == 0) flag[2] = bi;
     }
-    __syncthreads();
+    cta_sync();
     const int pv = flag[2];
     if (pv != j) {  // symmetric swap of rows / columns j and pv
       for (int c = tid; c < n; c += nt) {
@@ -267,7 +271,7 @@ static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *pe
         bc[j] = bc[pv];
         bc[pv] = t;
       }
-      __syncthreads();
+      cta_sync();
       for (int r = tid; r < n; r += nt) {
         const double t = B[(long)j * ldb + r];
         B[(long)j * ldb + r] = B[(long)pv * ldb + r];
@@ -278,7 +282,7 @@ static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *pe
         perm[j] = perm[pv];
         perm[pv] = t;
       }
-      __syncthreads();
+      cta_sync();
     }
     double d = B[(long)j * ldb + j];
     const bool bad = !(d > 0.0) || !isfinite(d);
@@ -286,7 +290,7 @@ static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *pe
     const double r = sqrt(d), inv = 1.0 / r;
     double *bj = B + (long)j * ldb;
     for (int i = j + 1 + tid; i < n; i += nt) vec[i] = bj[i] * inv;
-    __syncthreads();
+    cta_sync();
     if (tid == 0) {
       bj[j] = r;
       if (bad) flag[1] |= SBLETKF_ERR_NONFINITE;
@@ -297,11 +301,11 @@ static __device__ __noinline__ int chol_pivot(double *B, int n, int ldb, int *pe
       double *bc = B + (long)c * ldb;
       for (int i = j + 1 + tx; i < n; i += 16) bc[i] = fma(-vec[i], vc, bc[i]);
     }
-    __syncthreads();
+    cta_sync();
   }
   for (int c = ty; c < n; c += nty)
     for (int i = tx; i < c; i += 16) B[(long)c * ldb + i] = 0.0;
-  __syncthreads();
+  cta_sync();
   return flag[1];
 }
 
@@ -337,7 +341,7 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
       y[t] = (inb && cb < n && r < n) ? B[(long)cb * ldb + r] : 0.0;
     }
   }
-  __syncthreads();
+  cta_sync();
   const double tol2 = tol * tol, big2 = stop * stop;
   int sweep = 0;
   for (; sweep < maxsw; ++sweep) {
@@ -357,7 +361,7 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
       ny = __shfl_sync(0xffffffffu, b, lane & ~(G - 1));
     }
     if (tid == 0) *flag = 0;
-    __syncthreads();
+    cta_sync();
     int big = 0;
     for (int step = 0; step < n2; ++step) {
       const bool odd = (step & 1) == 0;
@@ -400,7 +404,7 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
           }
           if (gl == 0) NL[grp] = ny;
         }
-        __syncthreads();
+        cta_sync();
         if (inb && grp + 1 < ng) {
 #pragma unroll
           for (int t = 0; t < E; ++t) {
@@ -423,7 +427,7 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
           }
           if (gl == 0) NR[grp] = nx;
         }
-        __syncthreads();
+        cta_sync();
         if (inb) {
           const double *src = grp > 0 ? SR + (long)(grp - 1) * ldb : SL;
 #pragma unroll
@@ -438,9 +442,9 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
       // slot is rewritten only after the following step's barrier
     }
     if (big) *flag = 1;
-    __syncthreads();
+    cta_sync();
     const int rot = *flag;
-    __syncthreads();
+    cta_sync();
     if (!rot) break;
   }
   if (tid == 0) flag[3] = sweep;  // sweeps run (diagnostics)
@@ -448,12 +452,12 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
   // column (squared norm exactly 0: it never rotates), whose place takes the
   // column at position n
   if (tid == 0) flag[2] = -1;
-  __syncthreads();
+  cta_sync();
   if ((n & 1) && inb && gl == 0) {
     if (!(nx > 0.0)) flag[2] = 2 * grp;
     if (!(ny > 0.0)) flag[2] = 2 * grp + 1;
   }
-  __syncthreads();
+  cta_sync();
   const int zpos = flag[2];
   if (inb) {
 #pragma unroll
@@ -469,7 +473,7 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
       }
     }
   }
-  __syncthreads();
+  cta_sync();
   return sweep >= maxsw ? SBLETKF_ERR_EIG_NOCONV : 0;
 }
 
@@ -479,7 +483,7 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
 template <int EMAX>
 static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, double tol, double stop, int maxsw,
                                                  double *lam, int *flag, int *perm, double *vec) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = kThreads >> 5;
   int bits = chol_pivot(B, n, ldb, perm, vec, flag);
   if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, stop, maxsw, vec, flag);
   else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, stop, maxsw, vec, flag);
@@ -507,10 +511,10 @@ static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, doub
     }
   }
   if (threadIdx.x == 0) flag[1] = 0;
-  __syncthreads();
-  for (int j = threadIdx.x; j < n; j += blockDim.x)
+  cta_sync();
+  for (int j = threadIdx.x; j < n; j += kThreads)
     if (!(lam[j] > 0.0) || !isfinite(lam[j])) atomicOr(flag + 1, SBLETKF_ERR_NONFINITE);
-  __syncthreads();
+  cta_sync();
   bits |= flag[1];
   return bits;
 }
@@ -525,7 +529,7 @@ static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, doub
 template <int EMAX>
 static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb, double tol, double stop, int maxsw,
                                                       double *lam, int *flag, double *vec, const double *V, double *X) {
-  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+  const int tid = threadIdx.x, nt = kThreads, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
   // X = A V, 4 columns of V per thread pass (A symmetric, column q of A = row q)
   for (int e = tid; e < n * ((n + 3) / 4); e += nt) {
     const int r = e % n, c0 = (e / n) * 4;
@@ -543,9 +547,9 @@ static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb,
     if (c0 + 2 < n) X[(long)(c0 + 2) * n + r] = s2;
     if (c0 + 3 < n) X[(long)(c0 + 3) * n + r] = s3;
   }
-  __syncthreads();
+  cta_sync();
   for (int e = tid; e < n * n; e += nt) B[(long)(e / n) * ldb + (e % n)] = X[e];
-  __syncthreads();
+  cta_sync();
   int bits = 0;
   if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, stop, maxsw, vec, flag);
   else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, stop, maxsw, vec, flag);
@@ -572,10 +576,10 @@ static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb,
     }
   }
   if (threadIdx.x == 0) flag[1] = 0;
-  __syncthreads();
-  for (int j = threadIdx.x; j < n; j += blockDim.x)
+  cta_sync();
+  for (int j = threadIdx.x; j < n; j += kThreads)
     if (!(lam[j] > 0.0) || !isfinite(lam[j])) atomicOr(flag + 1, SBLETKF_ERR_NONFINITE);
-  __syncthreads();
+  cta_sync();
   bits |= flag[1];
   return bits;
 }
@@ -584,7 +588,7 @@ static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb,
 // column j, lanes over rows m (contiguous in a column of V).
 static __device__ __forceinline__ void x_times_v(const double *X, int ldx, int nv, const double *V, int n, int ldb,
                                                  double *out, int ldo) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = kThreads >> 5;
   for (int j = wid; j < n; j += nw) {
     const double *vj = V + (long)j * ldb;
     double acc[kNvMax];
@@ -608,7 +612,7 @@ static __device__ __forceinline__ void x_times_v(const double *X, int ldx, int n
 
 // out[j] = sum_m V[m][j] x[m] (j < n), warp per column, lanes over rows.
 static __device__ __forceinline__ void vt_times(const double *V, int n, int ldb, const double *x, double *out) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = kThreads >> 5;
   for (int j = wid; j < n; j += nw) {
     const double *vj = V + (long)j * ldb;
     double s = 0.0;
@@ -626,9 +630,9 @@ __device__ __forceinline__ void pf_weights(const PointSmem &S, int k) {
     for (int j = 1; j < k; ++j) mx = S.ll[j] > mx ? S.ll[j] : mx;
     S.misc[40] = mx;
   }
-  __syncthreads();
+  cta_sync();
   if (threadIdx.x < k) S.ll[threadIdx.x] = exp(__dsub_rn(S.ll[threadIdx.x], S.misc[40]));
-  __syncthreads();
+  cta_sync();
   if (threadIdx.x == 0) {
     double s = 0.0;
     for (int j = 0; j < k; ++j) s = __dadd_rn(s, S.ll[j]);
@@ -639,7 +643,7 @@ __device__ __forceinline__ void pf_weights(const PointSmem &S, int k) {
       S.cw[j] = acc;
     }
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // First i with r <= cw[i] (i < k-1), else k-1 (common_lpfgm.f90:142-149).
@@ -717,7 +721,7 @@ __device__ __forceinline__ void resample_draw(const sbletkf_params &p, const dou
 // (common_da.f90:354-401).  Mean into misc[v], spread into misc[8+v].
 __device__ __forceinline__ void mean_spread_pert(const PointSmem &S, int kp, int k, int nvt) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int v = wid; v < nvt; v += blockDim.x >> 5) {
+  for (int v = wid; v < nvt; v += kThreads >> 5) {
     double *xv = S.x + v * kp;
     double s = 0.0;
     for (int m = lane; m < k; m += 32) s += xv[m];
@@ -734,7 +738,7 @@ __device__ __forceinline__ void mean_spread_pert(const PointSmem &S, int kp, int
       S.misc[8 + v] = sp;
     }
   }
-  __syncthreads();
+  cta_sync();
 }
 
 // RTPP / RTPS on the analysis in S.an (rows v < nvt) with forecast
@@ -743,7 +747,7 @@ __device__ __forceinline__ void mean_spread_pert(const PointSmem &S, int kp, int
 __device__ __forceinline__ void relax_and_clamp(const sbletkf_params &p, const PointSmem &S, int kp, int k, int nvt,
                                                 int kl, double phi) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int v = wid; v < nvt; v += blockDim.x >> 5) {
+  for (int v = wid; v < nvt; v += kThreads >> 5) {
     double *av = S.an + v * kp;
     const double *dxf = S.x + v * kp;
     double s = 0.0;
@@ -771,7 +775,7 @@ __device__ __forceinline__ void relax_and_clamp(const sbletkf_params &p, const P
       av[m] = a;
     }
   }
-  __syncthreads();
+  cta_sync();
 }
 
 }  // namespace sbl

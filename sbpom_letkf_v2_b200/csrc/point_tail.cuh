@@ -45,7 +45,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       const int o = e / KP, m = e - o * KP;
       Z[o * ldz + m] = ob.hdxf64[(long)S.lidx[o] * ob.ldh + m];
     }
-    __syncthreads();
+    cta_sync();
     if (do_pf && tid < k) {
       double ll = llv;
       for (int o = 0; o < n; ++o) {
@@ -56,13 +56,13 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       }
       llv = ll;
     }
-    __syncthreads();
+    cta_sync();
     for (int e = tid; e < n * KP; e += kThreads) {
       const int o = e / KP, m = e - o * KP;
       Z[o * ldz + m] *= sqrt(S.lw[o]);
     }
     if (tid < n) S.b[tid] = sqrt(S.lw[tid]) * S.ldep[tid];
-    __syncthreads();
+    cta_sync();
     for (int e = tid; e < n * n; e += kThreads) {  // N = alpha I + Z Z^T
       const int r = e % n, c = e / n;
       if (r <= c) {
@@ -73,11 +73,11 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
         Nb[(long)r * ldn + c] = s;
       }
     }
-    __syncthreads();
+    cta_sync();
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
     bits |= jacobi_eig<(KP / 4 < 16 ? KP / 4 : 16)>(Nb, n, ldn, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
     vt_times(Nb, n, ldn, S.b, S.c);  // c = Lambda^-1 Q^T d
-    __syncthreads();
+    cta_sync();
     if (tid < n) S.c[tid] /= S.lam[tid];
   }
   if (!dual && nacc > 0 && do_gram) {
@@ -91,7 +91,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       warm = 1;
     }
     vt_times(S.u, k, S.ldb, S.b, S.c);  // c = Lambda^-1 V^T b
-    __syncthreads();
+    cta_sync();
     if (tid < k) S.c[tid] /= S.lam[tid];
   }
   if (do_pf && tid < k) S.ll[tid] = llv;
@@ -104,7 +104,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
     else xv = (double)f2[((long)(v - p.nv3d) * k + m) * nij1 + i];
     S.x[v * KP + m] = xv;
   }
-  __syncthreads();
+  cta_sync();
   mean_spread_pert(S, KP, k, nvt);
 
   const double *B = S.u;
@@ -117,7 +117,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       for (int m = 0; m < k; ++m) s = fma(xv[m], zo[m], s);
       S.t[v * KP + o] = s;
     }
-    __syncthreads();
+    cta_sync();
     for (int e = tid; e < nvt * n; e += kThreads) {  // Pq = P Q
       const int v = e / n, j = e - v * n;
       const double *qj = Nb + (long)j * ldn, *pv = S.t + v * KP;
@@ -125,7 +125,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       for (int o = 0; o < n; ++o) s = fma(pv[o], qj[o], s);
       S.w[v * KP + j] = s;
     }
-    __syncthreads();
+    cta_sync();
     {
       const int lane = tid & 31, wid = tid >> 5;
       for (int v = wid; v < nvt; v += kThreads / 32) {  // dX wvec = Pq Lambda^-1 Q^T d
@@ -135,14 +135,14 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
         if (lane == 0) S.misc[16 + v] = s;
       }
     }
-    __syncthreads();
+    cta_sync();
     const double sa = sqrt(alpha_d);
     for (int e = tid; e < nvt * n; e += kThreads) {
       const int v = e / n, j = e - v * n;
       const double lj = S.lam[j];
       S.w[v * KP + j] *= letkf ? -1.0 / (sqrt(alpha_d * lj) * (sqrt(lj) + sa)) : 1.0 / lj;
     }
-    __syncthreads();
+    cta_sync();
     for (int e = tid; e < nvt * n; e += kThreads) {  // Sq = (Pq g) Q^T
       const int v = e / n, o = e - v * n;
       const double *wv = S.w + v * KP;
@@ -150,7 +150,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       for (int j = 0; j < n; ++j) s = fma(wv[j], Nb[(long)j * ldn + o], s);
       S.t[v * KP + o] = s;
     }
-    __syncthreads();
+    cta_sync();
     // LETKF: anal = xm + dX wvec + sqrt(k-1) (alpha^-1/2 dX + Sq Z)
     // LPFGM: U = dX W_GM = (dX w) 1^T + dX - (dX Z^T Q Lambda^-1 Q^T) Z
     const double sk = sqrt((double)(k - 1)), isa = 1.0 / sa;
@@ -163,10 +163,10 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       if (letkf) S.an[v * KP + m] = S.misc[v] + S.misc[16 + v] + sk * (isa * dx + s);
       else S.w[v * KP + m] = S.misc[16 + v] + dx - s;
     }
-    __syncthreads();
+    cta_sync();
   } else if (nacc > 0 && do_gram) {
     x_times_v(S.x, KP, nvt, B, k, S.ldb, S.t, KP);  // T = dX V
-    __syncthreads();
+    cta_sync();
     {  // mean increment dX wvec = T c (LETKF), or dX w_gm (LPFGM)
       const int lane = tid & 31, wid = tid >> 5;
       for (int v = wid; v < nvt; v += kThreads / 32) {
@@ -176,14 +176,14 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
         if (lane == 0) S.misc[16 + v] = s;
       }
     }
-    __syncthreads();
+    cta_sync();
     const bool letkf = p.iswitch_da == SBLETKF_DA_LETKF;
     for (int e = tid; e < nvt * k; e += kThreads) {
       const int v = e / k, j = e - v * k;
       const double lj = S.lam[j];
       S.t[v * KP + j] *= letkf ? sqrt((double)(k - 1) / lj) : 1.0 / lj;
     }
-    __syncthreads();
+    cta_sync();
     // LETKF: anal = xm + dX wvec + T2 V^T
     // LPFGM: U = dX W_GM = (dX w) 1^T + alpha dX Pa  (W_GM = w 1^T + alpha Pa,
     //        equal to I + Pa (R^-1 Y)^T (dep 1^T - Y) of gm_core, common_lpfgm.f90:384-397)
@@ -196,7 +196,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       for (int j = 0; j < k; ++j) s = fma(tv[j], B[(long)j * S.ldb + m], s);
       dst[v * KP + m] = letkf ? S.misc[v] + S.misc[16 + v] + s : S.misc[16 + v] + agm * s;
     }
-    __syncthreads();
+    cta_sync();
   } else if (!do_pf || nacc == 0) {
     // letkf_core_noobs: W = sqrt(rho) I ; lpfgm_core_noobs: W = I
     const double d = (p.iswitch_da == SBLETKF_DA_LETKF) ? sqrt(p.cov_infl_mul) : 1.0;
@@ -204,7 +204,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       const int v = e / k, m = e - v * k;
       S.an[v * KP + m] = S.misc[v] + S.x[v * KP + m] * d;
     }
-    __syncthreads();
+    cta_sync();
   }
 
   if (do_pf && nacc > 0) {
@@ -219,7 +219,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
     for (int e = tid; e < nvt * k; e += kThreads) S.an[(e / k) * KP + e % k] = 0.0;
     for (int d0 = 0; d0 < p.nmonte; d0 += kDrawBatch) {
       const int nb = min(kDrawBatch, p.nmonte - d0);
-      __syncthreads();
+      cta_sync();
       for (int t = wid; t < nb; t += kThreads / 32) {  // a warp per draw
         const int d = d0 + t;
         const double *u = (p.rm == SBLETKF_RM_SR) ? uni + pid * p.nmonte + d : uni + (pid * p.nmonte + d) * k;
@@ -230,7 +230,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
           for (int j = lane; j < k; j += 32) so[j] = sr[j];
         }
       }
-      __syncthreads();
+      cta_sync();
       for (int e = tid; e < nvt * k; e += kThreads) {
         const int v = e / k, j = e - v * k;
         double s = S.an[v * KP + j];
@@ -238,13 +238,13 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
         S.an[v * KP + j] = s;
       }
     }
-    __syncthreads();
+    cta_sync();
     const double inv = 1.0 / (double)p.nmonte;
     for (int e = tid; e < nvt * k; e += kThreads) {
       const int v = e / k, j = e - v * k;
       S.an[v * KP + j] = S.misc[v] + S.an[v * KP + j] * inv;
     }
-    __syncthreads();
+    cta_sync();
   }
 
   // ---- RTPP / RTPS / round-off, then store
@@ -258,9 +258,9 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
   if (tc_on && (bits & SBLETKF_ERR_TIMEOUT)) atomicOr(status, SBLETKF_ERR_TIMEOUT);
   __shared__ int s_bits;
   if (tid == 0) s_bits = 0;
-  __syncthreads();
+  cta_sync();
   if (bits) atomicOr(&s_bits, bits);
-  __syncthreads();
+  cta_sync();
   bits = s_bits;
   if (tid == 0) {
     if (pst) pst[pid] = bits;

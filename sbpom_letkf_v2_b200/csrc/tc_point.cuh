@@ -97,7 +97,7 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const RowLoader &ro
   }
   rows(stg, f, cnt);
   if (tid < kKC) sw[tid] = tid < cnt ? (float)sqrt(S.lw[f + tid]) : 0.0f;
-  __syncthreads();
+  cta_sync();
   st.broken = s_broken;
   if (!st.broken && (st.nchunk & 1) && st.nchunk >= 3) {  // pair (nchunk - 3) / 2 is complete: add it
     fence_after_sync();
@@ -125,7 +125,7 @@ __device__ __forceinline__ void tc_chunk(const PointSmem &S, const RowLoader &ro
     store_split8(stage, tile_off(m, g * 8), z);
   }
   fence_async_smem();
-  __syncthreads();
+  cta_sync();
   if (tid == 0 && !st.broken) {
     fence_after_sync();
     const uint32_t idesc = idesc_bf16(kM, KP);
@@ -169,7 +169,7 @@ __device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint6
       }
     s_brk = brk;
   }
-  __syncthreads();
+  cta_sync();
   st.broken = s_brk;
   fence_after_sync();
   if (!st.broken)
@@ -193,7 +193,7 @@ __device__ __forceinline__ void tc_finish(const PointSmem &S, TcState &st, uint6
   }
   if (tid < k) S.b[tid] = bacc;
   fence_before_sync();
-  __syncthreads();
+  cta_sync();
 }
 
 // Tensor-memory columns of one CTA: sum hi, sum lo and two chunk-pair
@@ -218,7 +218,7 @@ __device__ __forceinline__ void tc_open(TcState &st, uint64_t *mbar, uint32_t *s
     tc::mbar_init(&mbar[1], 1);
   }
   tc::fence_before_sync();
-  __syncthreads();
+  cta_sync();
   tc::fence_after_sync();
   st.tbase = *s_tmem;
 }
@@ -242,7 +242,7 @@ __device__ __forceinline__ void tc_close(TcState &st, uint64_t *mbar, int *statu
     s_free = ok;
   }
   tc::fence_before_sync();
-  __syncthreads();
+  cta_sync();
   if (s_free && (threadIdx.x >> 5) == 0) {
     tc::fence_after_sync();
     tc::tmem_dealloc(st.tbase, tc_cols<KP>());

@@ -3,7 +3,9 @@
 Two knobs change speed but not the analysis (beyond rounding, and the mixed
 path's stated error):
 
-* the schedule: the persistent column queue with warm-started eigensolves
+* the schedule: the pipelined column queue (``Analysis.SCHED_PIPELINE``,
+  producer warps selecting the next point while consumer warps solve the
+  current one), the persistent column queue with warm-started eigensolves
   (``Analysis.SCHED_COLUMNS``) or one CTA per grid point
   (``Analysis.SCHED_POINT``); the warm start pays off where points need the
   k x k eigensolve, not for the LPF;
@@ -50,10 +52,19 @@ def _store(path, table):
     os.replace(tmp, path)
 
 
-def candidates(params):
+def schedules(params):
+    """The launch schedules that apply: the pipelined column queue needs an
+    eigensolve (not the LPF) and nmem <= 112."""
     from .analysis import Analysis
+    out = [Analysis.SCHED_COLUMNS, Analysis.SCHED_POINT]
+    if params.iswitch_da != 2 and params.nmem <= 112:
+        out.insert(0, Analysis.SCHED_PIPELINE)
+    return out
+
+
+def candidates(params):
     tcs = TC_CANDIDATES if (params.precision == 1 and params.iswitch_da != 2) else (0.0,)
-    return [{"schedule": s, "tc_max_cand": t} for s in (Analysis.SCHED_COLUMNS, Analysis.SCHED_POINT) for t in tcs]
+    return [{"schedule": s, "tc_max_cand": t} for s in schedules(params) for t in tcs]
 
 
 def column_sample(grid: dict, fcst3d, fcst2d, uniforms, nlev: int, max_cols: int):

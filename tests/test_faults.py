@@ -79,7 +79,7 @@ def test_point_status_marks_the_failing_points(cuda):
     an.close()
 
 
-@pytest.mark.parametrize("schedule", [Analysis.SCHED_COLUMNS, Analysis.SCHED_POINT])
+@pytest.mark.parametrize("schedule", [Analysis.SCHED_PIPELINE, Analysis.SCHED_COLUMNS, Analysis.SCHED_POINT])
 def test_prelatched_timeout_aborts_mixed_launch_and_context_stays_usable(schedule, cuda):
     """The path every tensor-core launch takes once a bounded wait has expired
     somewhere: with SBLETKF_ERR_TIMEOUT latched on the host before the launch,

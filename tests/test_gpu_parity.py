@@ -195,28 +195,33 @@ def test_mixed_dense_points_route_to_fp64_gram(cuda):
     assert em <= TOL_MIXED and es <= TOL_MIXED
 
 
-@pytest.mark.parametrize("k,precision", [(20, 0), (64, 0), (100, 0), (100, 1)])
-def test_both_schedules_match_the_oracle(k, precision, cuda):
-    """One CTA per point (every eigensolve cold) and the persistent column
-    queue (eigensolves warm-started from the level above) agree with the
-    oracle and with each other."""
+@pytest.mark.parametrize("k,precision", [(20, 0), (64, 0), (100, 0), (100, 1), (64, 1), (20, 1)])
+def test_all_schedules_match_the_oracle(k, precision, cuda):
+    """One CTA per point (every eigensolve cold), the persistent column queue
+    (eigensolves warm-started from the level above) and the pipelined column
+    queue (next point's selection and Gram overlapped with this point's
+    eigensolve) agree with the oracle and with each other."""
     case = _case(k, cov_infl_mul=1.1, alpha_rtps=0.4)
     g, ob, f3, f2 = _np(case)
     ref = cref.da_main(case.params, g, ob, f3, f2, rsize=8)
     p = case.params.replace(precision=precision)
     r0 = run_gpu(p, g, ob, f3, f2, schedule=Analysis.SCHED_POINT)
     r1 = run_gpu(p, g, ob, f3, f2, schedule=Analysis.SCHED_COLUMNS)
+    r2 = run_gpu(p, g, ob, f3, f2, schedule=Analysis.SCHED_PIPELINE)
     tol = TOL64 if precision == 0 else TOL_MIXED
-    for r in (r0, r1):
+    for r in (r0, r1, r2):
         assert (r["status"] == 0).all()
+        assert np.array_equal(r["nobsl"], ref["nobsl"])
         assert field_relerr(r["anal3d"], ref["anal3d"]) <= tol
         assert field_relerr(r["anal2d"], ref["anal2d"]) <= tol
     # warm and cold eigensolves round differently: far below the 1e-10 parity bound
     assert field_relerr(r1["anal3d"], r0["anal3d"]) <= (1e-11 if precision == 0 else 1e-6)
+    # the FP64 pipeline accumulates the same Gram in the same order as the column queue
+    assert field_relerr(r2["anal3d"], r1["anal3d"]) <= (1e-11 if precision == 0 else 1e-6)
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_column_queue_with_multi_column_items(precision, cuda):
+@pytest.mark.parametrize("precision,schedule", [(0, 1), (1, 1), (0, 2), (1, 2)])
+def test_column_queue_with_multi_column_items(precision, schedule, cuda):
     """A grid wide enough that the column queue hands out items of several
     columns one latitude row apart (38,400 columns: 8 per item on a 148-SM
     B200, at least 2 on any GPU with up to 600 SMs).  Outputs start as NaN, so
@@ -229,7 +234,7 @@ def test_column_queue_with_multi_column_items(precision, cuda):
     p = case.params.replace(precision=precision)
     dev = "cuda:0"
     an = Analysis(p, case.nij1, ob["elm"].size, device=dev)
-    an.set_schedule(Analysis.SCHED_COLUMNS)
+    an.set_schedule(schedule)
     an.prepare_obs({k: torch.as_tensor(v, device=dev) for k, v in ob.items()})
     gt = {k: torch.as_tensor(v, device=dev, dtype=torch.float64) for k, v in g.items()}
     a3 = torch.full(f3.shape, float("nan"), dtype=torch.float64, device=dev)

@@ -20,8 +20,10 @@ def _case(precision=1):
 def test_candidates_and_key():
     case, p = _case(1)
     c = tune.candidates(p)
-    assert len(c) == 2 * len(tune.TC_CANDIDATES)
-    assert len(tune.candidates(p.replace(precision=0))) == 2
+    assert len(c) == 3 * len(tune.TC_CANDIDATES)          # pipeline, columns, point x tc routing
+    assert len(tune.candidates(p.replace(precision=0))) == 3
+    assert len(tune.candidates(p.replace(nmem=120))) == 2 * len(tune.TC_CANDIDATES)   # no pipeline above 112
+    assert len(tune.candidates(p.replace(iswitch_da=2, precision=0))) == 2
     assert tune.key(p, "B200") != tune.key(p.replace(nmem=32), "B200")
 
 
@@ -48,7 +50,7 @@ def test_cache_round_trip_and_fastest_choice(tmp_path):
     path = str(tmp_path / "tune.json")
     r = tune.tune(p, case.grid, case.fcst3d, case.fcst2d, case.obs, cache=path, gpu_name="X", measure=fake)
     assert r["schedule"] == 0 and r["tc_max_cand"] == 0.0
-    assert len(r["ms"]) == len(calls) - 2                # the failing candidate is dropped
+    assert len(r["ms"]) == len(calls) - 3                # the failing candidates are dropped
     n = len(calls)
     r2 = tune.tune(p, case.grid, case.fcst3d, case.fcst2d, case.obs, cache=path, gpu_name="X", measure=fake)
     assert len(calls) == n and r2 == r                   # served from the cache
@@ -61,7 +63,7 @@ def test_gpu_tuning_choice_reproduces_the_analysis(tmp_path, cuda):
     case, p = _case(1)
     c = case.to("cuda:0")
     cfg = tune.tune(p, c.grid, c.fcst3d, c.fcst2d, c.obs, cache=str(tmp_path / "t.json"))
-    assert cfg["schedule"] in (0, 1) and len(cfg["ms"]) >= 1
+    assert cfg["schedule"] in (0, 1, 2) and len(cfg["ms"]) >= 1
     outs = []
     for use in (None, cfg):
         an = Analysis(p, c.nij1, c.obs["elm"].numel(), device="cuda:0")
