@@ -216,8 +216,9 @@ def test_all_schedules_match_the_oracle(k, precision, cuda):
         assert field_relerr(r["anal2d"], ref["anal2d"]) <= tol
     # warm and cold eigensolves round differently: far below the 1e-10 parity bound
     assert field_relerr(r1["anal3d"], r0["anal3d"]) <= (1e-11 if precision == 0 else 1e-6)
-    # the FP64 pipeline accumulates the same Gram in the same order as the column queue
-    assert field_relerr(r2["anal3d"], r1["anal3d"]) <= (1e-11 if precision == 0 else 1e-6)
+    # FP64: the pipeline accumulates the same Gram in the same order as the column queue;
+    # mixed: both within 1e-4 of the oracle, with chunk pairs of 64 and 128 observations
+    assert field_relerr(r2["anal3d"], r1["anal3d"]) <= (1e-11 if precision == 0 else 1e-5)
 
 
 @pytest.mark.parametrize("precision,schedule", [(0, 1), (1, 1), (0, 2), (1, 2)])
