@@ -499,9 +499,9 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying CUDA graphs")
     ap.add_argument("--tune", action="store_true",
                     help="pick schedule and tensor-core routing with the autotuner before timing")
-    ap.add_argument("--schedule", choices=["pipeline", "columns", "point"], default="pipeline",
-                    help="pipelined column queue (producer / consumer warps), persistent column queue with "
-                         "warm-started eigensolves, or one CTA per point (the LPF always uses its default)")
+    ap.add_argument("--schedule", choices=["auto", "pipeline", "columns", "point"], default="auto",
+                    help="auto (pipelined column queue for the mixed path, column queue for FP64, one CTA per "
+                         "point for the LPF), or one of those for every path (the LPF always uses its default)")
     ap.add_argument("--no-aux", action="store_true",
                     help="skip the timing of the observation operator and the ensemble statistics")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -568,7 +568,7 @@ def main():
         uni = uni.reshape(P_local, *uni_full.shape[1:]).contiguous()
 
     an = Analysis(p, ncol, nobs, device=dev)
-    sched = {"pipeline": Analysis.SCHED_PIPELINE, "columns": Analysis.SCHED_COLUMNS,
+    sched = {"auto": Analysis.SCHED_AUTO, "pipeline": Analysis.SCHED_PIPELINE, "columns": Analysis.SCHED_COLUMNS,
              "point": Analysis.SCHED_POINT}[args.schedule]
     if not pf:   # the LPF keeps its default (one CTA per point)
         an.set_schedule(sched)

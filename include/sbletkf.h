@@ -273,21 +273,26 @@ int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const vo
                                  void *stream);
 
 /* Launch schedule of sbletkf_analysis for this workspace.
+ * SBLETKF_SCHED_AUTO (the default): SBLETKF_SCHED_PIPELINE for the mixed
+ * path where it applies, SBLETKF_SCHED_COLUMNS for the FP64 path (whose
+ * Gram runs on the consumer warps and is faster in the 256-thread CTA),
+ * SBLETKF_SCHED_POINT for the LPF.
  * SBLETKF_SCHED_COLUMNS: one persistent 256-thread CTA per SM takes items of
  * up to 8 grid columns, nlon apart (neighbours along a meridian), from an
  * atomic queue and walks their levels in snake order, starting every k x k
  * eigensolve from the eigenvectors of the previous one; items narrow to 1
  * column when the grid has fewer than 32 items of 8 per CTA.
- * SBLETKF_SCHED_PIPELINE (the default for LETKF and LPFGM with nmem <= 112):
- * the same walk by a warp-specialised 384-thread CTA per SM, whose 4 producer
+ * SBLETKF_SCHED_PIPELINE (LETKF and LPFGM with nmem <= 112; otherwise the
+ * column queue runs): the same walk by a warp-specialised 384-thread CTA per SM, whose 4 producer
  * warps select the local observations of the next point (and, mixed
  * precision, accumulate its Gram on the tensor cores) while its 8 consumer
  * warps run the eigensolve and update of the current one.  The workspace
  * then holds two local-obs lists of max_nobs entries per SM (12 bytes each).
- * SBLETKF_SCHED_POINT (the LPF default, which has no eigensolve): one CTA per
- * grid point.  All give the same analysis to rounding.
+ * SBLETKF_SCHED_POINT: one CTA per grid point (the LPF has no eigensolve to
+ * warm-start).  All give the same analysis to rounding.
  * No reference counterpart (the reference's OpenMP DYNAMIC loop over (k,i),
  * common_da.f90:66-68, is the scheduling it replaces). */
+#define SBLETKF_SCHED_AUTO     (-1)
 #define SBLETKF_SCHED_POINT    0
 #define SBLETKF_SCHED_COLUMNS  1
 #define SBLETKF_SCHED_PIPELINE 2

@@ -62,14 +62,15 @@ class Analysis:
         self._keep = []
         self.nobs = None
 
-    SCHED_POINT, SCHED_COLUMNS, SCHED_PIPELINE = 0, 1, 2
+    SCHED_AUTO, SCHED_POINT, SCHED_COLUMNS, SCHED_PIPELINE = -1, 0, 1, 2
 
     def set_schedule(self, schedule: int) -> None:
-        """SCHED_PIPELINE (default for LETKF / LPFGM, nmem <= 112): the column
-        walk with the next point's selection and Gram (producer warps)
-        overlapped with the current point's eigensolve and update (consumer
-        warps); SCHED_COLUMNS: persistent column queue with warm-started
-        eigensolves; SCHED_POINT: one CTA per grid point."""
+        """SCHED_AUTO (default): SCHED_PIPELINE for the mixed path, SCHED_COLUMNS
+        for FP64, SCHED_POINT for the LPF.  SCHED_PIPELINE (LETKF / LPFGM,
+        nmem <= 112): the column walk with the next point's selection and Gram
+        (producer warps) overlapped with the current point's eigensolve and
+        update (consumer warps); SCHED_COLUMNS: persistent column queue with
+        warm-started eigensolves; SCHED_POINT: one CTA per grid point."""
         _abi.check(self.lib.sbletkf_workspace_set_schedule(self._ws, int(schedule)), "set_schedule")
 
     # -- lifetime ---------------------------------------------------------

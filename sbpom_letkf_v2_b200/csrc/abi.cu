@@ -93,14 +93,12 @@ int sbletkf_workspace_create(const sbletkf_params *p, int32_t nij1, int32_t max_
     ws->nslab = nsm;
     alloc((void **)&ws->d_queue, sizeof(int32_t) * 4);
     alloc((void **)&ws->d_slab, sizeof(double) * 2 * (size_t)p->nmem * p->nmem * (size_t)(nsm > 0 ? nsm : 1));
-    // the LPF has no eigensolve to warm-start: one CTA per point suits it
-    ws->schedule = p->iswitch_da == SBLETKF_DA_LPF ? SBLETKF_SCHED_POINT : SBLETKF_SCHED_COLUMNS;
+    ws->schedule = SBLETKF_SCHED_AUTO;
     if (pipeline_supported(p)) {  // the pipelined schedule's per-CTA local-obs lists
       ws->list_cap = (long long)no;
       const size_t nl = (size_t)2 * (size_t)(nsm > 0 ? nsm : 1) * (size_t)ws->list_cap;
       alloc((void **)&ws->d_list_idx, sizeof(int32_t) * nl);
       alloc((void **)&ws->d_list_rloc, sizeof(double) * nl);
-      ws->schedule = SBLETKF_SCHED_PIPELINE;
     }
   }
   if (e == cudaSuccess) e = cudaMallocHost((void **)&ws->h_status, sizeof(int32_t) * 4);
@@ -174,8 +172,8 @@ int sbletkf_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const sblet
 }
 
 int sbletkf_workspace_set_schedule(sbletkf_workspace *ws, int32_t schedule) {
-  if (!ws || (schedule != SBLETKF_SCHED_POINT && schedule != SBLETKF_SCHED_COLUMNS &&
-              schedule != SBLETKF_SCHED_PIPELINE))
+  if (!ws || (schedule != SBLETKF_SCHED_AUTO && schedule != SBLETKF_SCHED_POINT &&
+              schedule != SBLETKF_SCHED_COLUMNS && schedule != SBLETKF_SCHED_PIPELINE))
     return SBLETKF_ERR_ARG;
   if (schedule == SBLETKF_SCHED_PIPELINE && !ws->d_list_idx) return SBLETKF_ERR_UNSUPPORTED;
   ws->schedule = schedule;

@@ -401,13 +401,16 @@ int launch_t(const sbletkf_params *p, const GridView &g, const ObsView &ob, cons
 int launch_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, const void *f3,
                     const void *f2, void *a3, void *a2, int dtype, const double *uni, int32_t *src, int32_t *pst,
                     cudaStream_t s) {
-  if (ws->schedule == SBLETKF_SCHED_PIPELINE && ws->d_list_idx && ws->d_queue && ws->d_slab &&
-      pipeline_supported(p))
+  int sched = ws->schedule;
+  if (sched == SBLETKF_SCHED_AUTO)
+    sched = p->iswitch_da == SBLETKF_DA_LPF     ? SBLETKF_SCHED_POINT
+            : p->precision == SBLETKF_PREC_MIXED ? SBLETKF_SCHED_PIPELINE
+                                                 : SBLETKF_SCHED_COLUMNS;
+  if (sched == SBLETKF_SCHED_PIPELINE && ws->d_list_idx && ws->d_queue && ws->d_slab && pipeline_supported(p))
     return launch_analysis_ws(ws, p, g, f3, f2, a3, a2, dtype, uni, src, pst, s);
   const ObsView ob = ws->obs_view();
   Sched sc{nullptr, nullptr, 0};
-  if (ws->schedule >= SBLETKF_SCHED_COLUMNS && ws->d_queue && ws->d_slab)
-    sc = Sched{ws->d_queue, ws->d_slab, ws->nslab};
+  if (sched >= SBLETKF_SCHED_COLUMNS && ws->d_queue && ws->d_slab) sc = Sched{ws->d_queue, ws->d_slab, ws->nslab};
   if (dtype == SBLETKF_F64) return launch_t<double>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, sc, s);
   return launch_t<float>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, sc, s);
 }

@@ -155,8 +155,9 @@ struct sbletkf_workspace {
   int32_t *d_status;
   int32_t *h_status;  // pinned
   double *d_gscratch; // backward scalar accumulators [2]
-  // analysis schedule: 0 = one CTA per point, 1 = persistent column queue
-  // with warm-started eigensolves (d_queue counter, d_slab 2 k x k FP64 per CTA)
+  // analysis schedule (SBLETKF_SCHED_*): -1 automatic, 0 one CTA per point,
+  // 1 persistent column queue with warm-started eigensolves (d_queue counter,
+  // d_slab 2 k x k FP64 per CTA), 2 the pipelined column queue
   int schedule = 0;
   int nslab = 0;
   int32_t *d_queue = nullptr;
