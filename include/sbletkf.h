@@ -263,6 +263,23 @@ int sbletkf_obs_operator(const sbletkf_params *p, const double *glon, const doub
                          const sbletkf_obs_in *obs, int32_t flags, const sbletkf_obs_out *out, double *stats,
                          void *stream);
 
+/* Observation-space monitors: monit_mean (common.f90:681-840) and
+ * monit_sprd (:846-978), which write_ens_mpi applies to H(mean) and
+ * H(spread) of the forecast and of the analysis (common_io.f90:1039-1045).
+ * For every observation whose hx[o] is defined (not NaN, the reference's
+ * undef) the value v = dat[o] - hx[o] (SBLETKF_MONIT_DEPARTURE; dat may be
+ * NULL otherwise) or v = hx[o] (SBLETKF_MONIT_VALUE) is added to
+ * stats[(ivd*3 + c)*3 + j]: ivd the variable of the element id (iv3d_u,
+ * iv3d_v, iv3d_t, iv3d_s; SSH nv3d + iv2d_z), c = 0 all, 1 surface
+ * (lev == 0), 2 interior (3D variables only), j = 0 count, 1 sum of v,
+ * 2 sum of v^2.  stats ([(nv3d+nv2d)*9] FP64, device) is added to: zero it
+ * first.  Bias = sum/count, RMSD = sqrt(sum of squares/count), spread =
+ * sum/count.  Asynchronous. */
+#define SBLETKF_MONIT_DEPARTURE 0
+#define SBLETKF_MONIT_VALUE     1
+int sbletkf_obs_monitor(const sbletkf_params *p, int32_t nobs, const int32_t *elm, const double *lev,
+                        const double *dat, const double *hx, int32_t mode, double *stats, void *stream);
+
 /* Ensemble mean and spread (k-1) of a state, per variable, level and point
  * (ensemble_mesp, common.f90:505-596): state3d [nv3d][nmem][nlev][nij1] ->
  * mean3d / sprd3d [nv3d][nlev][nij1], state2d [nv2d][nmem][nij1] -> mean2d /

@@ -197,3 +197,36 @@ def set_obs(p, g, obs, s3, s2, gross_qc=False, aoei=True):
         if aoei and qc[o] == 1:                        # common_obs.f90:385-397
             err[o] = math.sqrt(max(err[o] * err[o], dep[o] * dep[o] - sprd[o] * sprd[o]))
     return dict(idx=idx, idy=idy, qc=qc, hxmean=mean, hxsprd=sprd, hdxf=hdxf, dep=dep, err=err)
+
+
+def monit_sums(p, obs, hx, departure):
+    """monit_mean (common.f90:681-840, departure=True: v = dat - hx) and
+    monit_sprd (:846-978, v = hx): for every observation with hx defined
+    (not None / NaN), count, sum v and sum v^2 under its variable, and for the
+    3D variables under surface (lev == 0) or interior.  Serial, in
+    observation order.  Returns [nv3d+nv2d][all, surface, interior][count,
+    sum, sum of squares]."""
+    nvt = p.nv3d + p.nv2d
+    st = np.zeros((nvt, 3, 3))
+    vmap = {2819: p.iv3d_u, 2820: p.iv3d_v, 3073: p.iv3d_t, 3332: p.iv3d_s, p.id_z_obs: p.nv3d + p.iv2d_z}
+    for o in range(len(obs["elm"])):
+        h = hx[o]
+        if h is UNDEF or h is None or (isinstance(h, float) and math.isnan(h)):
+            continue
+        e = int(obs["elm"][o])
+        if e not in vmap:
+            continue
+        ivd = vmap[e]
+        v = obs["dat"][o] - h if departure else h
+        st[ivd, 0] += (1.0, v, v * v)
+        if e == p.id_z_obs:
+            continue
+        st[ivd, 1 if obs["lev"][o] == 0.0 else 2] += (1.0, v, v * v)
+    return st
+
+
+def hx_of_field(p, g, obs, f3, f2):
+    """Trans_XtoY of one state field f3 [nv3d][nlev][ncell], f2 [nv2d][ncell]
+    (write_ens_mpi, common_io.f90:967-985): a list with UNDEF where undefined."""
+    idx, idy = obs_id_uniform(obs["lon"], obs["lat"], g["lon"], g["lat"], p.nlon, p.nlat)
+    return trans_xtoy(p, g, obs, idx, idy, np.asarray(f3)[:, None], np.asarray(f2)[:, None], 0)

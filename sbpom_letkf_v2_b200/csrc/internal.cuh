@@ -199,6 +199,8 @@ int launch_core_batched(const sbletkf_params *p, int32_t npts, const int64_t *of
 int launch_obs_operator(const sbletkf_params *p, const double *glon, const double *glat, const double *gfsm,
                         const double *gdepth, const void *s3, const void *s2, int dtype, const sbletkf_obs_in *obs,
                         int flags, const sbletkf_obs_out *out, double *stats, cudaStream_t s);
+int launch_obs_monitor(const sbletkf_params *p, int nobs, const int32_t *elm, const double *lev, const double *dat,
+                       const double *hx, int mode, double *stats, cudaStream_t s);
 int launch_ens_mesp(const sbletkf_params *p, int nij1, const void *s3, const void *s2, int dtype, void *m3, void *sd3,
                     void *m2, void *sd2, cudaStream_t s);
 int launch_backward(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, const void *f3,

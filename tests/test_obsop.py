@@ -117,3 +117,67 @@ def test_obs_operator_feeds_the_analysis(cuda):
     e3 = np.abs(a3.cpu().numpy() - a_ref["anal3d"]).max() / np.abs(a_ref["anal3d"]).max()
     e2 = np.abs(a2.cpu().numpy() - a_ref["anal2d"]).max() / np.abs(a_ref["anal2d"]).max()
     assert e3 <= 1e-10 and e2 <= 1e-10
+
+
+# ---- observation-space monitors (monit_mean / monit_sprd) --------------------
+
+def test_monit_sums_known_answers():
+    """The restatement of monit_mean / monit_sprd on a hand-made set: undef
+    hx and unknown elements are skipped, SSH has no surface / interior split."""
+    from sbpom_letkf_v2_b200.params import LETKFParams
+    p = LETKFParams(nmem=4, nlon=4, nlat=4, nlev=6, nv3d=4, nv2d=1)
+    obs = dict(elm=[3073, 3073, 3332, 2567, 3073, 9999], lev=[0.0, -10.0, -5.0, 0.0, 0.0, 0.0],
+               dat=[10.0, 11.0, 35.0, 0.5, 9.0, 1.0])
+    hx = [9.0, 8.0, 34.5, 0.25, None, 3.0]
+    st = OO.monit_sums(p, obs, hx, True)
+    t, s, z = p.iv3d_t, p.iv3d_s, p.nv3d + p.iv2d_z
+    assert st[t].tolist() == [[2, 4.0, 10.0], [1, 1.0, 1.0], [1, 3.0, 9.0]]
+    assert st[s].tolist() == [[1, 0.5, 0.25], [0, 0, 0], [1, 0.5, 0.25]]
+    assert st[z].tolist() == [[1, 0.25, 0.0625], [0, 0, 0], [0, 0, 0]]
+    assert st.sum() == st[[t, s, z]].sum()
+    sp = OO.monit_sums(p, obs, hx, False)
+    assert sp[t, 0].tolist() == [2, 17.0, 145.0]
+
+
+@pytest.mark.gpu
+def test_write_ens_monitors_match_the_oracle(cuda):
+    """The monitors write_ens_mpi prints (common_io.f90:917-1045) on the GPU:
+    ensemble mean / spread fields of the forecast and of an analysis, H of
+    each, monit_mean (O-B, O-A) and monit_sprd; against the restatement:
+    counts exact, H and the sums within 1e-12 relative."""
+    from sbpom_letkf_v2_b200.obsop import MONIT_DEPARTURE, MONIT_VALUE, obs_monitor, write_ens_monitors
+    case, p, grid, obs = _raw_case(k=12, nobs=400, seed=5)
+    f3, f2 = case.fcst3d.double(), case.fcst2d.double()
+    a3 = 0.6 * f3 + 0.4 * f3.mean(1, keepdim=True) + 0.01      # an analysis-like state: spread shrunk, mean moved
+    a2 = 0.6 * f2 + 0.4 * f2.mean(1, keepdim=True) - 0.02
+    dev = "cuda:0"
+    gt = {k: torch.as_tensor(v, device=dev) for k, v in grid.items()}
+    ot = {k: torch.as_tensor(v, device=dev) for k, v in obs.items()}
+    res = write_ens_monitors(p, gt, ot, f3.to(dev), f2.to(dev), a3.to(dev), a2.to(dev))
+    k = p.nmem
+    for name, s3, s2 in (("fcst", f3, f2), ("anal", a3, a2)):
+        x3, x2 = s3.numpy(), s2.numpy()
+        m3, m2 = x3.mean(1), x2.mean(1)
+        d3 = np.sqrt(((x3 - m3[:, None]) ** 2).sum(1) / (k - 1))
+        d2 = np.sqrt(((x2 - m2[:, None]) ** 2).sum(1) / (k - 1))
+        for key, f3f, f2f, mode in (("hxmean", m3, m2, MONIT_DEPARTURE), ("hxsprd", d3, d2, MONIT_VALUE)):
+            ref = OO.hx_of_field(p, grid, obs, f3f, f2f)
+            want = np.array([np.nan if h is None else h for h in ref])
+            got = res[name][key].cpu().numpy()
+            assert np.array_equal(np.isnan(got), np.isnan(want))
+            ok = ~np.isnan(want)
+            assert 0 < ok.sum() < ok.size
+            assert np.abs(got[ok] - want[ok]).max() <= TOL * np.abs(want[ok]).max()
+            st = obs_monitor(p, ot, res[name][key], mode).cpu().numpy()
+            sr = OO.monit_sums(p, obs, ref, mode == MONIT_DEPARTURE)
+            assert np.array_equal(st[..., 0], sr[..., 0])
+            for j in (1, 2):
+                assert np.abs(st[..., j] - sr[..., j]).max() <= TOL * max(1.0, np.abs(sr[..., j]).max())
+        m, s = res[name]["mean"], res[name]["sprd"]
+        sr = OO.monit_sums(p, obs, OO.hx_of_field(p, grid, obs, m3, m2), True)
+        n = sr[..., 0]
+        with np.errstate(invalid="ignore", divide="ignore"):
+            bias = np.where(n > 0, sr[..., 1] / n, np.nan)
+        assert np.array_equal(m["n"].numpy(), n.astype(np.int64))
+        assert np.allclose(m["bias"].numpy(), bias, rtol=1e-12, atol=1e-14, equal_nan=True)
+        assert s["n"].sum() > 0
