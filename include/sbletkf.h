@@ -315,6 +315,12 @@ int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const vo
 #define SBLETKF_SCHED_PIPELINE 2
 int sbletkf_workspace_set_schedule(sbletkf_workspace *ws, int32_t schedule);
 
+/* Columns per item of the column queue (SBLETKF_SCHED_COLUMNS and _PIPELINE):
+ * 0 (the default) picks 8 when the grid gives at least 32 items of 8 per
+ * CTA and narrower otherwise; 1..8 fixes it (the autotuner's knob).  Any
+ * width gives the same analysis to rounding.  No reference counterpart. */
+int sbletkf_workspace_set_item_width(sbletkf_workspace *ws, int32_t width);
+
 /* Vector-Jacobian product of the LETKF analysis (iswitch_da = 1, with RTPP,
  * RTPS and the T/S round-off): given dJ/d anal3d and dJ/d anal2d (same layouts
  * as the state, state_dtype), accumulate dJ/d dep and dJ/d rdiag ([nobs],

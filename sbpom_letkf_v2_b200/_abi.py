@@ -29,7 +29,7 @@ EXPORTS = ("sbletkf_abi_version", "sbletkf_workspace_create", "sbletkf_workspace
            "sbletkf_prepare_obs", "sbletkf_analysis", "sbletkf_count_nobsl", "sbletkf_get_status",
            "sbletkf_core_batched", "sbletkf_backward", "sbletkf_analysis_noalloc",
            "sbletkf_obs_operator", "sbletkf_ensemble_mean_spread", "sbletkf_workspace_set_schedule",
-           "sbletkf_latch_status", "sbletkf_obs_monitor")
+           "sbletkf_latch_status", "sbletkf_obs_monitor", "sbletkf_workspace_set_item_width")
 NOALLOC_MAX_OBS, NOALLOC_MAX_CELLS = 8192, 65536
 
 
@@ -92,6 +92,7 @@ def load(path: str = LIB_PATH):
         "sbletkf_workspace_set_schedule": ([vp, i32], ctypes.c_int),
         "sbletkf_latch_status": ([vp, i32, vp], ctypes.c_int),
         "sbletkf_obs_monitor": ([pp, i32, vp, vp, vp, vp, i32, vp, vp], ctypes.c_int),
+        "sbletkf_workspace_set_item_width": ([vp, i32], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -73,6 +73,10 @@ class Analysis:
         warm-started eigensolves; SCHED_POINT: one CTA per grid point."""
         _abi.check(self.lib.sbletkf_workspace_set_schedule(self._ws, int(schedule)), "set_schedule")
 
+    def set_item_width(self, width: int) -> None:
+        """Columns per column-queue item (0: automatic, 1..8)."""
+        _abi.check(self.lib.sbletkf_workspace_set_item_width(self._ws, int(width)), "set_item_width")
+
     # -- lifetime ---------------------------------------------------------
     def close(self) -> None:
         if self._ws:

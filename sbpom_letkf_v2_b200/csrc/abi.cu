@@ -180,6 +180,12 @@ int sbletkf_workspace_set_schedule(sbletkf_workspace *ws, int32_t schedule) {
   return SBLETKF_OK;
 }
 
+int sbletkf_workspace_set_item_width(sbletkf_workspace *ws, int32_t width) {
+  if (!ws || width < 0 || width > 8) return SBLETKF_ERR_ARG;
+  ws->item_width = width;
+  return SBLETKF_OK;
+}
+
 int sbletkf_count_nobsl(sbletkf_workspace *ws, const sbletkf_params *p, const sbletkf_grid *grid, int32_t *nobsl,
                         void *stream) {
   if (!ws || !ws->prepared || !nobsl) return SBLETKF_ERR_ARG;

@@ -348,6 +348,7 @@ struct Sched {
   int *queue;    // nullptr: one CTA per point
   double *slab;
   int ctas;
+  int width;     // columns per queue item
 };
 
 template <int R, typename ST, bool MIXED>
@@ -358,11 +359,7 @@ int launch_r(const sbletkf_params *p, const GridView &g, const ObsView &ob, cons
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_status(e);
   if (sc.queue) {
-    // Queue items of up to 8 columns; narrower when the grid has fewer than
-    // 32 items of 8 per CTA, because the dynamic queue balances the CTAs'
-    // loads only to within about one item.
-    const long long per = (long long)g.nij1 / ((long long)sc.ctas * 32);
-    const int colchunk = per >= 8 ? 8 : per < 1 ? 1 : (int)per;
+    const int colchunk = sc.width;
     const int cstride = p->nlon > 1 ? p->nlon : 1;
     e = cudaMemsetAsync(sc.queue, 0, sizeof(int), s);
     if (e != cudaSuccess) return cuda_status(e);
@@ -409,8 +406,9 @@ int launch_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const GridVi
   if (sched == SBLETKF_SCHED_PIPELINE && ws->d_list_idx && ws->d_queue && ws->d_slab && pipeline_supported(p))
     return launch_analysis_ws(ws, p, g, f3, f2, a3, a2, dtype, uni, src, pst, s);
   const ObsView ob = ws->obs_view();
-  Sched sc{nullptr, nullptr, 0};
-  if (sched >= SBLETKF_SCHED_COLUMNS && ws->d_queue && ws->d_slab) sc = Sched{ws->d_queue, ws->d_slab, ws->nslab};
+  Sched sc{nullptr, nullptr, 0, 1};
+  if (sched >= SBLETKF_SCHED_COLUMNS && ws->d_queue && ws->d_slab)
+    sc = Sched{ws->d_queue, ws->d_slab, ws->nslab, queue_item_width(ws, g.nij1, ws->nslab)};
   if (dtype == SBLETKF_F64) return launch_t<double>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, sc, s);
   return launch_t<float>(p, g, ob, f3, f2, a3, a2, uni, src, pst, ws->d_status, sc, s);
 }

@@ -761,8 +761,7 @@ int launch_ws_r(const sbletkf_params *p, const GridView &g, const ObsView &ob, c
   auto kern = k_analysis_ws<R, ST, MIXED>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_status(e);
-  const long long per = (long long)g.nij1 / ((long long)ws->nslab * 32);
-  const int colchunk = per >= 8 ? 8 : per < 1 ? 1 : (int)per;
+  const int colchunk = queue_item_width(ws, g.nij1, ws->nslab);
   const int cstride = p->nlon > 1 ? p->nlon : 1;
   e = cudaMemsetAsync(ws->d_queue, 0, sizeof(int), s);
   if (e != cudaSuccess) return cuda_status(e);

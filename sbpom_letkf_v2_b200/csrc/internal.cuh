@@ -159,6 +159,7 @@ struct sbletkf_workspace {
   // 1 persistent column queue with warm-started eigensolves (d_queue counter,
   // d_slab 2 k x k FP64 per CTA), 2 the pipelined column queue
   int schedule = 0;
+  int item_width = 0;  // columns per queue item: 0 automatic, else 1..8
   int nslab = 0;
   int32_t *d_queue = nullptr;
   double *d_slab = nullptr;
@@ -189,6 +190,14 @@ int launch_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const GridVi
 int launch_count(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, int32_t *nobsl,
                  cudaStream_t s);
 bool pipeline_supported(const sbletkf_params *p);
+// Columns per item of the column queue: the workspace's setting, or 8 when
+// the grid gives at least 32 such items per CTA, narrower otherwise (the
+// dynamic queue balances the CTAs only to within about one item).
+inline int queue_item_width(const sbletkf_workspace *ws, long long nij1, int ctas) {
+  if (ws->item_width > 0) return ws->item_width;
+  const long long per = nij1 / ((long long)ctas * 32);
+  return per >= 8 ? 8 : per < 1 ? 1 : (int)per;
+}
 int launch_analysis_ws(sbletkf_workspace *ws, const sbletkf_params *p, const GridView &g, const void *f3,
                        const void *f2, void *a3, void *a2, int dtype, const double *uni, int32_t *src, int32_t *pst,
                        cudaStream_t s);

@@ -10,7 +10,10 @@ path's stated error):
   (``Analysis.SCHED_POINT``); the warm start pays off where points need the
   k x k eigensolve, not for the LPF;
 * for the mixed path, ``tc_max_cand``: the search-box candidate count above
-  which a point's Gram is accumulated in FP64 instead of on the tensor cores.
+  which a point's Gram is accumulated in FP64 instead of on the tensor cores;
+* for the column-queue schedules, the queue-item width (columns per item,
+  ``Analysis.set_item_width``), timed on a block of whole latitude rows so
+  that the items' columns are real neighbours.
 
 ``tune`` times the candidates on a sample of the caller's own columns
 (every s-th column of the grid, all levels, the full observation set) with
@@ -90,6 +93,7 @@ def _gpu_measure(params, grid, fcst3d, fcst2d, obs, uniforms, cand, reps):
     an = Analysis(p, grid["lon1"].numel(), max(1, obs["elm"].numel()), device=fcst3d.device)
     try:
         an.set_schedule(cand["schedule"])
+        an.set_item_width(cand.get("item_width", 0))
         an.prepare_obs(obs)
         a3, a2 = torch.empty_like(fcst3d), torch.empty_like(fcst2d)
         an.da_main(grid, fcst3d, fcst2d, uniforms=uniforms, anal3d=a3, anal2d=a2, check=False)
@@ -108,10 +112,35 @@ def _gpu_measure(params, grid, fcst3d, fcst2d, obs, uniforms, cand, reps):
         an.close()
 
 
+def row_sample(grid: dict, fcst3d, fcst2d, uniforms, nlev: int, nlon: int, max_cols: int):
+    """A block of whole latitude rows from the middle of the grid (at most
+    max_cols columns): columns nlon apart stay neighbours, as the column
+    queue's items assume.  Grid arrays, state and (PF) uniforms of it."""
+    nij1 = grid["lon1"].numel()
+    nrow = nij1 // nlon
+    rows = max(1, min(nrow, max_cols // max(nlon, 1)))
+    c0 = (nrow - rows) // 2 * nlon
+    cols = torch.arange(c0, c0 + rows * nlon, device=fcst3d.device)
+    g = {k: (v.index_select(v.dim() - 1, cols)).contiguous() for k, v in grid.items()}
+    f3 = fcst3d.index_select(3, cols).contiguous()
+    f2 = fcst2d.index_select(2, cols).contiguous()
+    uni = None
+    if uniforms is not None:
+        u = uniforms.view(nlev, nij1, *uniforms.shape[1:]).index_select(1, cols)
+        uni = u.reshape(nlev * cols.numel(), *uniforms.shape[1:]).contiguous()
+    return g, f3, f2, uni
+
+
+WIDTHS = (0, 1, 2, 4, 8)   # columns per queue item (0: the library's choice)
+
+
 def tune(params, grid: dict, fcst3d, fcst2d, obs: dict, uniforms=None, max_cols: int = 4096, reps: int = 2,
          cache: str | None = CACHE, force: bool = False, gpu_name: str | None = None, measure=None) -> dict:
-    """The fastest candidate for this workload: {"schedule", "tc_max_cand",
-    "ms": {candidate: time}}; read from / written to `cache` (None: no cache)."""
+    """The fastest configuration for this workload: {"schedule", "tc_max_cand",
+    "item_width", "ms": {candidate: time}, "ms_width": {width: time}}; read
+    from / written to `cache` (None: no cache).  Stage 1 times schedule x
+    tensor-core routing on a column sample; stage 2 times the queue-item
+    widths of the chosen queue schedule on a block of whole rows."""
     if gpu_name is None:
         gpu_name = torch.cuda.get_device_name(fcst3d.device) if fcst3d.is_cuda else "cpu"
     k = key(params, gpu_name)
@@ -128,7 +157,17 @@ def tune(params, grid: dict, fcst3d, fcst2d, obs: dict, uniforms=None, max_cols:
     if not times:
         raise RuntimeError("no candidate configuration completed without an error status")
     best = json.loads(min(times, key=times.get))
-    result = dict(best, ms=times, sample_columns=int(g["lon1"].numel()))
+    best["item_width"] = 0
+    wtimes = {}
+    if best["schedule"] != 0:   # a column-queue schedule: tune its item width
+        gr, r3, r2, ur = row_sample(grid, fcst3d, fcst2d, uniforms, params.nlev, params.nlon, max_cols)
+        for wd in WIDTHS:
+            t = measure(params, gr, r3, r2, obs, ur, dict(best, item_width=wd), reps)
+            if t is not None:
+                wtimes[str(wd)] = t
+        if wtimes:
+            best["item_width"] = int(min(wtimes, key=wtimes.get))
+    result = dict(best, ms=times, ms_width=wtimes, sample_columns=int(g["lon1"].numel()))
     if cache:
         table = _load(cache)
         table[k] = result
@@ -137,6 +176,8 @@ def tune(params, grid: dict, fcst3d, fcst2d, obs: dict, uniforms=None, max_cols:
 
 
 def apply(analysis, params, cfg: dict):
-    """Set the tuned schedule on `analysis`; return the parameters to use."""
+    """Set the tuned schedule and item width on `analysis`; return the
+    parameters to use."""
     analysis.set_schedule(int(cfg["schedule"]))
+    analysis.set_item_width(int(cfg.get("item_width", 0)))
     return params.replace(tc_max_cand=float(cfg["tc_max_cand"]))

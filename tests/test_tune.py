@@ -51,6 +51,7 @@ def test_cache_round_trip_and_fastest_choice(tmp_path):
     r = tune.tune(p, case.grid, case.fcst3d, case.fcst2d, case.obs, cache=path, gpu_name="X", measure=fake)
     assert r["schedule"] == 0 and r["tc_max_cand"] == 0.0
     assert len(r["ms"]) == len(calls) - 3                # the failing candidates are dropped
+    assert r["ms_width"] == {}                           # one CTA per point: no queue items to size
     n = len(calls)
     r2 = tune.tune(p, case.grid, case.fcst3d, case.fcst2d, case.obs, cache=path, gpu_name="X", measure=fake)
     assert len(calls) == n and r2 == r                   # served from the cache
@@ -74,3 +75,23 @@ def test_gpu_tuning_choice_reproduces_the_analysis(tmp_path, cuda):
         an.close()
     m0, m1 = outs[0].mean(axis=1), outs[1].mean(axis=1)
     assert np.abs(m1 - m0).max() <= 1e-4 * np.abs(m0).max()
+
+
+def test_item_width_stage_and_row_sample():
+    """When a queue schedule wins, stage 2 times the item widths on whole
+    latitude rows and keeps the fastest."""
+    case, p = _case()
+    calls = []
+
+    def fake(params, g, f3, f2, obs, uni, cand, reps):
+        calls.append((cand, g["lon1"].numel()))
+        if "item_width" in cand:
+            return 5.0 + abs(cand["item_width"] - 2)        # width 2 is fastest
+        return 10.0 - cand["schedule"] + cand["tc_max_cand"] / 1e4   # the pipeline (2) wins
+    r = tune.tune(p, case.grid, case.fcst3d, case.fcst2d, case.obs, cache=None, gpu_name="X", measure=fake)
+    assert r["schedule"] == 2 and r["item_width"] == 2 and set(r["ms_width"]) == {str(w) for w in tune.WIDTHS}
+    g, f3, f2, _ = tune.row_sample(case.grid, case.fcst3d, case.fcst2d, None, p.nlev, p.nlon, 3 * p.nlon + 5)
+    n = g["lon1"].numel()
+    assert n == 3 * p.nlon and f3.shape[-1] == n and g["depth1"].shape == (p.nlev, n)
+    assert torch.equal(g["rj1"].view(3, p.nlon)[:, 0].diff(), torch.ones(2, dtype=g["rj1"].dtype))
+    assert all(w == case.nij1 for c, w in calls if "item_width" in c)   # a small grid: every row
