@@ -38,12 +38,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 METRIC = "analysis gridpoints/s per LETKF cycle, mixed vs FP64 on B200 at <=1e-4 rel err"
 TC_MAX_CAND_DEFAULT = 12288.0   # library default of sbletkf_params.tc_max_cand
 
-# DRAM bytes per analysed point of k_analysis (read + written), from one ncu
-# capture of the same launch shape: workload 1 on its full horizontal grid
-# with 2 levels (bench.py --levels 2), which gets the same 8-column queue
-# items, mixed path.  Scaled by the points of a launch.
-DRAM_BYTES_PER_POINT_W1 = 1073.6e6 / 240000.0
-DRAM_SCHEDULE_W1 = "columns"      # the schedule that capture ran
+# DRAM bytes per analysed point of the mixed-path analysis kernel (read +
+# written), from ncu captures; scaled by the points of a launch.
+#   column queue: workload 1 on its full horizontal grid with 2 levels
+#     (bench.py --levels 2), which gets the same 8-column queue items;
+#   pipelined kernel: workload 1 on its 1/8 grid (bench.py --scale 8).
+DRAM_BYTES_PER_POINT_W1 = {"columns": 1073.6e6 / 240000.0, "pipeline": 278.9e6 / 74000.0}
 # The same for the LPF: workload 4 on its 1/2 grid (bench.py --workload 4 --scale 2).
 DRAM_BYTES_PER_POINT_W4 = 280.6e6 / 61440.0
 
@@ -743,8 +743,9 @@ def main():
             tmax = p.tc_max_cand if p.tc_max_cand > 0 else TC_MAX_CAND_DEFAULT
             tmask = np.broadcast_to((cand <= tmax)[None, :], (p.nlev, ncol)) if prec == PREC_MIXED else None
             fl = algorithmic_flops(nob_l, p.nmem, p.nv3d, p.nv2d, p.nlev, ncol, tmask)
-            traffic = (DRAM_BYTES_PER_POINT_W1 * P_local if (args.workload == 1 and prec == PREC_MIXED
-                                                            and args.schedule == DRAM_SCHEDULE_W1) else None)
+            run_sched = "pipeline" if args.schedule == "auto" else args.schedule
+            traffic = (DRAM_BYTES_PER_POINT_W1[run_sched] * P_local
+                       if (args.workload == 1 and prec == PREC_MIXED and run_sched in DRAM_BYTES_PER_POINT_W1) else None)
             roof = letkf_roofline(fl, kern_ms, _fp64_peak(dev), peaks, src, traffic)
         cpu = None
         chk = None
