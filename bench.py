@@ -500,8 +500,9 @@ def main():
     ap.add_argument("--tune", action="store_true",
                     help="pick schedule and tensor-core routing with the autotuner before timing")
     ap.add_argument("--schedule", choices=["auto", "pipeline", "columns", "point"], default="auto",
-                    help="auto (pipelined column queue for the mixed path, column queue for FP64, one CTA per "
-                         "point for the LPF), or one of those for every path (the LPF always uses its default)")
+                    help="auto (pipelined column queue for the mixed path with 65 <= k <= 112, column queue "
+                         "otherwise, one CTA per point for the LPF), or one of those for every path (the LPF "
+                         "always uses its default)")
     ap.add_argument("--no-aux", action="store_true",
                     help="skip the timing of the observation operator and the ensemble statistics")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -743,7 +744,8 @@ def main():
             tmax = p.tc_max_cand if p.tc_max_cand > 0 else TC_MAX_CAND_DEFAULT
             tmask = np.broadcast_to((cand <= tmax)[None, :], (p.nlev, ncol)) if prec == PREC_MIXED else None
             fl = algorithmic_flops(nob_l, p.nmem, p.nv3d, p.nv2d, p.nlev, ncol, tmask)
-            run_sched = "pipeline" if args.schedule == "auto" else args.schedule
+            run_sched = (("pipeline" if 65 <= p.nmem <= 112 else "columns") if args.schedule == "auto"
+                         else args.schedule)
             traffic = (DRAM_BYTES_PER_POINT_W1[run_sched] * P_local
                        if (args.workload == 1 and prec == PREC_MIXED and run_sched in DRAM_BYTES_PER_POINT_W1) else None)
             roof = letkf_roofline(fl, kern_ms, _fp64_peak(dev), peaks, src, traffic)

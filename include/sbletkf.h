@@ -291,8 +291,9 @@ int sbletkf_ensemble_mean_spread(const sbletkf_params *p, int32_t nij1, const vo
 
 /* Launch schedule of sbletkf_analysis for this workspace.
  * SBLETKF_SCHED_AUTO (the default): SBLETKF_SCHED_PIPELINE for the mixed
- * path where it applies, SBLETKF_SCHED_COLUMNS for the FP64 path (whose
- * Gram runs on the consumer warps and is faster in the 256-thread CTA),
+ * path with 65 <= nmem <= 112 (where a point's eigensolve outweighs the
+ * producer's tensor-core Gram), SBLETKF_SCHED_COLUMNS for the other LETKF /
+ * LPFGM cases (the FP64 Gram is faster in the 256-thread CTA),
  * SBLETKF_SCHED_POINT for the LPF.
  * SBLETKF_SCHED_COLUMNS: one persistent 256-thread CTA per SM takes items of
  * up to 8 grid columns, nlon apart (neighbours along a meridian), from an

@@ -65,8 +65,9 @@ class Analysis:
     SCHED_AUTO, SCHED_POINT, SCHED_COLUMNS, SCHED_PIPELINE = -1, 0, 1, 2
 
     def set_schedule(self, schedule: int) -> None:
-        """SCHED_AUTO (default): SCHED_PIPELINE for the mixed path, SCHED_COLUMNS
-        for FP64, SCHED_POINT for the LPF.  SCHED_PIPELINE (LETKF / LPFGM,
+        """SCHED_AUTO (default): SCHED_PIPELINE for the mixed path with
+        65 <= nmem <= 112, SCHED_COLUMNS for the other LETKF / LPFGM cases,
+        SCHED_POINT for the LPF.  SCHED_PIPELINE (LETKF / LPFGM,
         nmem <= 112): the column walk with the next point's selection and Gram
         (producer warps) overlapped with the current point's eigensolve and
         update (consumer warps); SCHED_COLUMNS: persistent column queue with

@@ -399,10 +399,15 @@ int launch_analysis(sbletkf_workspace *ws, const sbletkf_params *p, const GridVi
                     const void *f2, void *a3, void *a2, int dtype, const double *uni, int32_t *src, int32_t *pst,
                     cudaStream_t s) {
   int sched = ws->schedule;
+  // Automatic: the pipeline pays where a point's eigensolve outweighs the
+  // producer's tensor-core Gram, whose cost per chunk does not shrink with k
+  // (UMMA M is 128 rows): 65 <= k <= 112.  Measured: k = 100 503.6k vs 439.4k
+  // gridpoints/s for the column queue; k = 64 685k vs 843k; k = 20 1.67M vs
+  // 2.2M.  The FP64 Gram is faster in the column queue's 256-thread CTA.
   if (sched == SBLETKF_SCHED_AUTO)
-    sched = p->iswitch_da == SBLETKF_DA_LPF     ? SBLETKF_SCHED_POINT
-            : p->precision == SBLETKF_PREC_MIXED ? SBLETKF_SCHED_PIPELINE
-                                                 : SBLETKF_SCHED_COLUMNS;
+    sched = p->iswitch_da == SBLETKF_DA_LPF                                ? SBLETKF_SCHED_POINT
+            : (p->precision == SBLETKF_PREC_MIXED && r_for_k(p->nmem) == 7) ? SBLETKF_SCHED_PIPELINE
+                                                                            : SBLETKF_SCHED_COLUMNS;
   if (sched == SBLETKF_SCHED_PIPELINE && ws->d_list_idx && ws->d_queue && ws->d_slab && pipeline_supported(p))
     return launch_analysis_ws(ws, p, g, f3, f2, a3, a2, dtype, uni, src, pst, s);
   const ObsView ob = ws->obs_view();
