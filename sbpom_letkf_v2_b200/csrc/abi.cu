@@ -92,7 +92,7 @@ int sbletkf_workspace_create(const sbletkf_params *p, int32_t nij1, int32_t max_
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     ws->nslab = nsm;
     alloc((void **)&ws->d_queue, sizeof(int32_t) * 4);
-    alloc((void **)&ws->d_slab, sizeof(double) * 2 * (size_t)p->nmem * p->nmem * (size_t)(nsm > 0 ? nsm : 1));
+    alloc((void **)&ws->d_slab, sizeof(double) * (size_t)p->nmem * p->nmem * (size_t)(nsm > 0 ? nsm : 1));
     ws->schedule = SBLETKF_SCHED_AUTO;
     if (pipeline_supported(p)) {  // the pipelined schedule's per-CTA local-obs lists
       ws->list_cap = (long long)no;

@@ -35,7 +35,7 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
                                               const double *__restrict__ uni, int32_t *__restrict__ src_out,
                                               int32_t *__restrict__ pst, int *status, const PointSmem &S,
                                               TcState &tcs, uint64_t *s_mbar, bool tc_on, long long pid,
-                                              double *vprev, double *xtmp, int &warm) {
+                                              double *vprev, int &warm) {
   constexpr int KP = kp_of_r(R);
   const int k = p.nmem;
   const int tid = threadIdx.x;
@@ -226,7 +226,7 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
     else store_gram<R>(S, k, alpha, A);
   }
   point_tail<R, ST>(p, ob, f3, f2, a3, a2, uni, src_out, pst, status, S, pid, nij1, phi, nacc, dual, A.ll, bits,
-                    tc_on, vprev, xtmp, warm);
+                    tc_on, vprev, warm);
 }
 
 // One CTA per grid point (queue == nullptr; point p0 + blockIdx.x), or a
@@ -234,7 +234,7 @@ __device__ __forceinline__ void analyze_point(const sbletkf_params &p, const Gri
 // columns, cstride apart, from the atomic counter *queue and analysing their
 // levels in snake order,
 // warm-starting every primal eigensolve from the previous primal point
-// (slab: 2 k x k FP64 scratch matrices per CTA).
+// (slab: one k x k FP64 matrix per CTA, the previous eigenvectors).
 template <int R, typename ST, bool MIXED>
 __global__ void __launch_bounds__(kThreads, 1)
     k_analysis(const sbletkf_params p, const GridView g, const ObsView ob, const ST *__restrict__ f3,
@@ -279,8 +279,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   // from the level above or below.  Items q and q+1 hold adjacent columns of
   // the same latitude rows, so the CTAs running at the same time read and
   // write the same 32-byte sectors of the state at about the same time.
-  double *vprev = queue ? slab + (size_t)blockIdx.x * 2 * k * k : nullptr;
-  double *xtmp = queue ? vprev + (size_t)k * k : nullptr;
+  double *vprev = queue ? slab + (size_t)blockIdx.x * k * k : nullptr;
   __shared__ int s_item;
   int warm = 0, c0 = 0, w = 0, pos = 0, npos = 0;
   bool first = true;
@@ -311,7 +310,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       pid = p0 + blockIdx.x;
     }
     analyze_point<R, ST, MIXED>(p, g, ob, f3, f2, a3, a2, uni, src_out, pst, status, S, tcs, s_mbar, tc_on, pid,
-                                vprev, xtmp, warm);
+                                vprev, warm);
   }
   if (tc_on && !aborted) tc_close<KP>(tcs, s_mbar, status);
 }

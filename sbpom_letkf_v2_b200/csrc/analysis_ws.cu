@@ -658,8 +658,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   } else {
     // =========================== consumer ===========================
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kRegCons));
-    double *vprev = slab + (size_t)blockIdx.x * 2 * k * k;
-    double *xtmp = vprev + (size_t)k * k;
+    double *vprev = slab + (size_t)blockIdx.x * k * k;
     const double alpha = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
     int warm = 0;
     for (int seq = 0;; ++seq) {
@@ -739,7 +738,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         }
         const int i = (int)(pid % nij1);
         point_tail<R, ST>(p, ob, f3, f2, a3, a2, uni, src_out, pst, status, S, pid, nij1, g.phi1[i], nacc, dual,
-                          llv, bits, tc_on, vprev, xtmp, warm);
+                          llv, bits, tc_on, vprev, warm);
       }
       cta_sync();
       if (tid == 0) mbar_arrive(&ctl.empty[s]);

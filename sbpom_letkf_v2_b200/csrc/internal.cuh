@@ -157,7 +157,7 @@ struct sbletkf_workspace {
   double *d_gscratch; // backward scalar accumulators [2]
   // analysis schedule (SBLETKF_SCHED_*): -1 automatic, 0 one CTA per point,
   // 1 persistent column queue with warm-started eigensolves (d_queue counter,
-  // d_slab 2 k x k FP64 per CTA), 2 the pipelined column queue
+  // d_slab k x k FP64 per CTA), 2 the pipelined column queue
   int schedule = 0;
   int item_width = 0;  // columns per queue item: 0 automatic, else 1..8
   int nslab = 0;

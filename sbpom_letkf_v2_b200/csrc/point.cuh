@@ -526,37 +526,68 @@ static __device__ __forceinline__ int jacobi_eig(double *B, int n, int ldb, doub
   return bits;
 }
 
+// X = A V for the warm start, written over A in B.  Thread (rt, ct) keeps
+// rows rt + i nrt (i < 4, nrt = ceil(n/4)) of columns CT ct .. CT ct + CT-1
+// in registers, reading A from shared memory (consecutive threads,
+// consecutive rows) and V's columns from global memory (a warp's threads
+// share one or two column tiles, so those loads are broadcasts).  One
+// barrier, then the tiles replace A.  Needs ceil(n/4) ceil(n/CT) <= kThreads.
+template <int CT>
+static __device__ __forceinline__ void warm_product(double *B, int n, int ldb, const double *V) {
+  const int nrt = (n + 3) >> 2, rt = threadIdx.x % nrt, c0 = CT * (threadIdx.x / nrt);
+  const bool act = c0 < n;
+  double acc[4][CT];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < CT; ++j) acc[i][j] = 0.0;
+  if (act) {
+    const double *vc = V + (long)c0 * n;
+#pragma unroll 2
+    for (int q = 0; q < n; ++q) {
+      const double *aq = B + (long)q * ldb + rt;
+      double a[4], v[CT];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = rt + i * nrt < n ? aq[i * nrt] : 0.0;
+#pragma unroll
+      for (int j = 0; j < CT; ++j) v[j] = c0 + j < n ? vc[(long)j * n + q] : 0.0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < CT; ++j) acc[i][j] = fma(a[i], v[j], acc[i][j]);
+    }
+  }
+  cta_sync();
+  if (act) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = rt + i * nrt;
+      if (r >= n) continue;
+#pragma unroll
+      for (int j = 0; j < CT; ++j)
+        if (c0 + j < n) B[(long)(c0 + j) * ldb + r] = acc[i][j];
+    }
+  }
+  cta_sync();
+}
+
 // Eigenpairs of the SPD matrix in B from a starting orthogonal matrix V
 // (n x n in global memory, column j at V + j*n; the eigenvectors of a nearby
-// matrix): one-sided Jacobi on the columns of X = A V (X in global scratch,
-// then in B).  Since X X^T = A^2, the converged columns are lambda_j u_j:
+// matrix): one-sided Jacobi on the columns of X = A V (formed in place of
+// A).  Since X X^T = A^2, the converged columns are lambda_j u_j:
 // lambda_j = |column j|, u_j = column / lambda_j.  When A is close to the
 // matrix V came from, X starts nearly orthogonal and needs a few sweeps
 // instead of the cold solve's pivoted Cholesky and ~10 sweeps.
 template <int EMAX>
 static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb, double tol, double stop, int maxsw,
-                                                      double *lam, int *flag, double *vec, const double *V, double *X) {
-  const int tid = threadIdx.x, nt = kThreads, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
-  // X = A V, 4 columns of V per thread pass (A symmetric, column q of A = row q)
-  for (int e = tid; e < n * ((n + 3) / 4); e += nt) {
-    const int r = e % n, c0 = (e / n) * 4;
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    const double *v0 = V + (long)c0 * n;
-    for (int q = 0; q < n; ++q) {
-      const double a = B[(long)q * ldb + r];
-      s0 = fma(a, v0[q], s0);
-      if (c0 + 1 < n) s1 = fma(a, v0[n + q], s1);
-      if (c0 + 2 < n) s2 = fma(a, v0[2 * n + q], s2);
-      if (c0 + 3 < n) s3 = fma(a, v0[3 * n + q], s3);
-    }
-    X[(long)c0 * n + r] = s0;
-    if (c0 + 1 < n) X[(long)(c0 + 1) * n + r] = s1;
-    if (c0 + 2 < n) X[(long)(c0 + 2) * n + r] = s2;
-    if (c0 + 3 < n) X[(long)(c0 + 3) * n + r] = s3;
-  }
-  cta_sync();
-  for (int e = tid; e < n * n; e += nt) B[(long)(e / n) * ldb + (e % n)] = X[e];
-  cta_sync();
+                                                      double *lam, int *flag, double *vec, const double *V) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = kThreads >> 5;
+  // column tile of warm_product: ceil(n/4) ceil(n/CT) <= 256 for n <= 4 EMAX
+  if (n <= 64 || EMAX <= 16) warm_product<4>(B, n, ldb, V);
+  else if (n <= 80 || EMAX <= 20) warm_product<8>(B, n, ldb, V);
+  else if (n <= 100 || EMAX <= 25) warm_product<10>(B, n, ldb, V);
+  else if (n <= 112 || EMAX <= 28) warm_product<13>(B, n, ldb, V);
+  else warm_product<16>(B, n, ldb, V);
   int bits = 0;
   if (n <= 32 || EMAX <= 8) bits |= jacobi_sweeps_oe<8>(B, n, ldb, tol, stop, maxsw, vec, flag);
   else if (n <= 64 || EMAX <= 16) bits |= jacobi_sweeps_oe<(EMAX < 16 ? EMAX : 16)>(B, n, ldb, tol, stop, maxsw, vec, flag);

@@ -15,7 +15,7 @@ namespace sbl {
 // and S.b holds b = Y^T diag(rloc/rdiag) dep; for a dual point S.lidx,
 // S.lw, S.ldep, S.lrloc, S.lrdiag hold its nacc local observations.  llv:
 // this thread's PF log-likelihood accumulated so far (member tid < k).
-// vprev / xtmp / warm: the warm-start state of the column schedule (vprev
+// vprev / warm: the warm-start state of the column schedule (vprev
 // nullptr: cold eigensolves).  tc_on: the tensor cores ran this launch
 // (a timed-out wait in bits is latched into *status at once).
 template <int R, typename ST>
@@ -24,7 +24,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
                                            const double *__restrict__ uni, int32_t *__restrict__ src_out,
                                            int32_t *__restrict__ pst, int *status, const PointSmem &S,
                                            long long pid, int nij1, double phi, int nacc, bool dual, double llv,
-                                           int bits, bool tc_on, double *vprev, double *xtmp, int &warm) {
+                                           int bits, bool tc_on, double *vprev, int &warm) {
   constexpr int KP = kp_of_r(R);
   const int k = p.nmem;
   const int tid = threadIdx.x;
@@ -83,7 +83,7 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
   if (!dual && nacc > 0 && do_gram) {
     const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
     if (vprev && warm)  // start from the previous level's eigenvectors
-      bits |= jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.cw, vprev, xtmp);
+      bits |= jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.cw, vprev);
     else
       bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
     if (vprev) {  // keep this level's eigenvectors for the next one
