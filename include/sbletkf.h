@@ -105,8 +105,11 @@ typedef struct sbletkf_params {
                           use the FP64 Gram; <= 0: library default 12288   */
   double jacobi_stop;  /* the eigensolve ends after a sweep whose largest relative
                           rotation |b_p.b_q| / (|b_p||b_q|) was at most this;
-                          <= 0: library default 1e-10 (1e-7 saves a sweep
-                          but leaves ~1e-8 relative error in the analysis) */
+                          <= 0: library default, 1e-10 on the FP64 path (1e-7
+                          saves a sweep but leaves ~1e-8 relative error in the
+                          analysis) and 1e-5 on the mixed path, whose Gram is
+                          accurate to ~1e-6: the sweep that meets 1e-5 leaves
+                          eigen-residuals of ~1e-10 (quadratic convergence) */
   double reserved_d[1];
 } sbletkf_params;
 

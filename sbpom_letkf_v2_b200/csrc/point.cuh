@@ -21,10 +21,15 @@
 namespace sbl {
 
 // Relative rotation size that ends the Jacobi eigensolve (see
-// jacobi_sweeps_oe) unless sbletkf_params.jacobi_stop sets another.
+// jacobi_sweeps_oe) unless sbletkf_params.jacobi_stop sets another.  The
+// mixed path's Gram carries ~1e-6 relative error, so its eigensolve stops
+// earlier: the sweep whose rotations stay below 1e-5 leaves residuals of
+// ~1e-10 (Jacobi converges quadratically), far below the Gram's error, and
+// a warm-started solve takes 3 sweeps instead of 4.
 constexpr double kJacobiStop = 1e-10;
+constexpr double kJacobiStopMixed = 1e-5;
 __host__ __device__ inline double jacobi_stop_of(const sbletkf_params &p) {
-  return p.jacobi_stop > 0.0 ? p.jacobi_stop : kJacobiStop;
+  return p.jacobi_stop > 0.0 ? p.jacobi_stop : p.precision == SBLETKF_PREC_MIXED ? kJacobiStopMixed : kJacobiStop;
 }
 
 // R x R register tile per thread over a 16 x 16 thread grid: k <= 16*R.

@@ -92,7 +92,7 @@ class LETKFParams:
     pi: float = 4.0 * math.atan(1.0)  # :27
     jacobi_tol: float = 0.0         # 0 -> library default (k * eps)
     tc_max_cand: float = 0.0        # mixed path: FP64 Gram above this many box candidates (0 -> 12288)
-    jacobi_stop: float = 0.0        # end the eigensolve after a sweep with no relative rotation above this (0 -> 1e-10)
+    jacobi_stop: float = 0.0        # end the eigensolve after a sweep with no relative rotation above this (0 -> 1e-10 FP64, 1e-5 mixed)
 
     def __post_init__(self):
         if self.dist_zero is None:

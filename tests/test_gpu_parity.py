@@ -214,8 +214,10 @@ def test_all_schedules_match_the_oracle(k, precision, cuda):
         assert np.array_equal(r["nobsl"], ref["nobsl"])
         assert field_relerr(r["anal3d"], ref["anal3d"]) <= tol
         assert field_relerr(r["anal2d"], ref["anal2d"]) <= tol
-    # warm and cold eigensolves round differently: far below the 1e-10 parity bound
-    assert field_relerr(r1["anal3d"], r0["anal3d"]) <= (1e-11 if precision == 0 else 1e-6)
+    # warm and cold eigensolves round differently: far below the 1e-10 parity bound;
+    # mixed: the eigensolve stops after the sweep whose rotations stay below 1e-5, so a
+    # warm solve (3 sweeps) and a cold one (8) also differ in truncation, ~1e-6
+    assert field_relerr(r1["anal3d"], r0["anal3d"]) <= (1e-11 if precision == 0 else 1e-5)
     # FP64: the pipeline accumulates the same Gram in the same order as the column queue;
     # mixed: both within 1e-4 of the oracle, with chunk pairs of 64 and 128 observations
     assert field_relerr(r2["anal3d"], r1["anal3d"]) <= (1e-11 if precision == 0 else 1e-5)
