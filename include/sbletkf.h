@@ -100,7 +100,9 @@ typedef struct sbletkf_params {
   double smin, smax;   /* S round-off bounds         (:131)                   */
   double re;           /* earth radius [m]           (:28)                    */
   double pi;           /* (:27)                                               */
-  double jacobi_tol;   /* relative off-diagonal tolerance of the eigensolve   */
+  double jacobi_tol;   /* smallest relative rotation the eigensolve applies;
+                          <= 0: k * 2^-52 on the FP64 path, 1e-9 on the mixed
+                          path (three orders under its Gram's error)        */
   double tc_max_cand;  /* mixed path: points whose search box holds more candidates
                           use the FP64 Gram; <= 0: library default 12288   */
   double jacobi_stop;  /* the eigensolve ends after a sweep whose largest relative

@@ -298,8 +298,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (nacc > 0) {
     P1.u = S.V;
     store_gram<R>(P1, k, alpha, A);  // A -> S.V, b -> S.b
-    const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
-    bits |= jacobi_eig<KP / 4>(S.V, k, S.ldv, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.vec);
+    // the backward pass computes in FP64 whatever the forward precision:
+    // FP64 defaults of the rotation threshold and stopping rule
+    sbletkf_params p64 = p;
+    p64.precision = SBLETKF_PREC_FP64;
+    const double tol = jacobi_tol_of(p64, k);
+    bits |= jacobi_eig<KP / 4>(S.V, k, S.ldv, tol, jacobi_stop_of(p64), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.vec);
     vt_times(S.V, k, S.ldv, S.b, S.c);
     __syncthreads();
     if (tid < k) S.c[tid] /= S.lam[tid];                    // c = Lambda^-1 V^T b

@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const double alpha = (double)(k - 1) / (p.iswitch_da == SBLETKF_DA_LETKF ? p.cov_infl_mul : p.cov_infl_gm);
       if (tc_on) tc_finish<KP>(S, tcs, s_mbar, k, alpha, A.b, bits);
       else store_gram<R>(S, k, alpha, A);
-      const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
+      const double tol = jacobi_tol_of(p, k);
       bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
       vt_times(S.u, k, S.ldb, S.b, S.c);
       __syncthreads();

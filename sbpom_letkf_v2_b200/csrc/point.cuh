@@ -31,6 +31,16 @@ constexpr double kJacobiStopMixed = 1e-5;
 __host__ __device__ inline double jacobi_stop_of(const sbletkf_params &p) {
   return p.jacobi_stop > 0.0 ? p.jacobi_stop : p.precision == SBLETKF_PREC_MIXED ? kJacobiStopMixed : kJacobiStop;
 }
+// Smallest relative rotation the sweeps apply, unless sbletkf_params.jacobi_tol
+// sets another: k eps on the FP64 path; 1e-9 on the mixed path, where the
+// rotations below it (left as residual) are three orders under the Gram's
+// own error and only cost the last sweep time.
+constexpr double kJacobiTolMixed = 1e-9;
+__host__ __device__ inline double jacobi_tol_of(const sbletkf_params &p, int k) {
+  return p.jacobi_tol > 0.0 ? p.jacobi_tol
+         : p.precision == SBLETKF_PREC_MIXED ? kJacobiTolMixed
+                                             : (double)k * 2.220446049250313e-16;
+}
 
 // R x R register tile per thread over a 16 x 16 thread grid: k <= 16*R.
 __host__ __device__ constexpr int kp_of_r(int r) { return 16 * r; }
@@ -391,7 +401,11 @@ static __device__ __forceinline__ int jacobi_sweeps_oe(double *B, int n, int ldb
       if (act && g2 > tol2 * ab) {
         // the angle only has to shrink b_p.b_q: FP32 with approximate division
         const float zf = __fdividef((float)(ny - nx) * 0.5f, (float)ga);
-        const float tf = __fdividef(copysignf(1.0f, zf), fabsf(zf) + sqrtf(fmaf(zf, zf, 1.0f)));
+        // sqrt(1 + z^2): q rsqrt(q) (MUFU) up to |z| = 4096, beyond which it
+        // rounds to |z| in FP32 (capping |z| instead would over-rotate pairs
+        // of very different norms)
+        const float az = fabsf(zf), qa = fminf(az, 4096.0f), q = fmaf(qa, qa, 1.0f);
+        const float tf = __fdividef(copysignf(1.0f, zf), az + (az > 4096.0f ? az : q * rsqrtf(q)));
         const double tt = (double)tf;
         const double cs = rsqrt(fma(tt, tt, 1.0)), sn = cs * tt;
 #pragma unroll

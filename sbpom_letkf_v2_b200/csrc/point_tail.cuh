@@ -74,14 +74,14 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
       }
     }
     cta_sync();
-    const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
+    const double tol = jacobi_tol_of(p, k);
     bits |= jacobi_eig<(KP / 4 < 16 ? KP / 4 : 16)>(Nb, n, ldn, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
     vt_times(Nb, n, ldn, S.b, S.c);  // c = Lambda^-1 Q^T d
     cta_sync();
     if (tid < n) S.c[tid] /= S.lam[tid];
   }
   if (!dual && nacc > 0 && do_gram) {
-    const double tol = p.jacobi_tol > 0.0 ? p.jacobi_tol : (double)k * 2.220446049250313e-16;
+    const double tol = jacobi_tol_of(p, k);
     if (vprev && warm)  // start from the previous level's eigenvectors
       bits |= jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.cw, vprev);
     else
