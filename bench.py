@@ -43,7 +43,7 @@ TC_MAX_CAND_DEFAULT = 12288.0   # library default of sbletkf_params.tc_max_cand
 #   column queue: workload 1 on its full horizontal grid with 2 levels
 #     (bench.py --levels 2), which gets the same 8-column queue items;
 #   pipelined kernel: workload 1 on its 1/8 grid (bench.py --scale 8).
-DRAM_BYTES_PER_POINT_W1 = {"columns": 1073.6e6 / 240000.0, "pipeline": 278.9e6 / 74000.0}
+DRAM_BYTES_PER_POINT_W1 = {"columns": 1073.6e6 / 240000.0, "pipeline": 258.6e6 / 74000.0}
 # The same for the LPF: workload 4 on its 1/2 grid (bench.py --workload 4 --scale 2).
 DRAM_BYTES_PER_POINT_W4 = 280.6e6 / 61440.0
 
