@@ -737,7 +737,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           cta_sync();
         }
         const int i = (int)(pid % nij1);
-        point_tail<R, ST>(p, ob, f3, f2, a3, a2, uni, src_out, pst, status, S, pid, nij1, g.phi1[i], nacc, dual,
+        point_tail<R, ST, true>(p, ob, f3, f2, a3, a2, uni, src_out, pst, status, S, pid, nij1, g.phi1[i], nacc, dual,
                           llv, bits, tc_on, vprev, warm);
       }
       cta_sync();

@@ -641,6 +641,15 @@ static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb,
   return bits;
 }
 
+// jacobi_eig_warm as a call of its own: the sweeps then get a register
+// allocation of their own instead of sharing it with the caller's live state
+// (the pipelined kernel's consumer runs at 192 registers per thread).
+template <int EMAX>
+static __device__ __noinline__ int jacobi_eig_warm_call(double *B, int n, int ldb, double tol, double stop, int maxsw,
+                                                        double *lam, int *flag, double *vec, const double *V) {
+  return jacobi_eig_warm<EMAX>(B, n, ldb, tol, stop, maxsw, lam, flag, vec, V);
+}
+
 // out[v*ldo + j] = sum_m X[v*ldx + m] V[m][j] for v < nv, j < n: warp per
 // column j, lanes over rows m (contiguous in a column of V).
 static __device__ __forceinline__ void x_times_v(const double *X, int ldx, int nv, const double *V, int n, int ldb,

@@ -18,7 +18,7 @@ namespace sbl {
 // vprev / warm: the warm-start state of the column schedule (vprev
 // nullptr: cold eigensolves).  tc_on: the tensor cores ran this launch
 // (a timed-out wait in bits is latched into *status at once).
-template <int R, typename ST>
+template <int R, typename ST, bool EIG_CALL = false>
 __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsView &ob, const ST *__restrict__ f3,
                                            const ST *__restrict__ f2, ST *__restrict__ a3, ST *__restrict__ a2,
                                            const double *__restrict__ uni, int32_t *__restrict__ src_out,
@@ -83,7 +83,10 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
   if (!dual && nacc > 0 && do_gram) {
     const double tol = jacobi_tol_of(p, k);
     if (vprev && warm)  // start from the previous level's eigenvectors
-      bits |= jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.cw, vprev);
+      bits |= EIG_CALL ? jacobi_eig_warm_call<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam,
+                                                      S.iws + 40, S.cw, vprev)
+                       : jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40,
+                                                 S.cw, vprev);
     else
       bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
     if (vprev) {  // keep this level's eigenvectors for the next one
