@@ -641,6 +641,13 @@ static __device__ __forceinline__ int jacobi_eig_warm(double *B, int n, int ldb,
   return bits;
 }
 
+// jacobi_eig as a call of its own (see jacobi_eig_warm_call).
+template <int EMAX>
+static __device__ __noinline__ int jacobi_eig_call(double *B, int n, int ldb, double tol, double stop, int maxsw,
+                                                   double *lam, int *flag, int *perm, double *vec) {
+  return jacobi_eig<EMAX>(B, n, ldb, tol, stop, maxsw, lam, flag, perm, vec);
+}
+
 // jacobi_eig_warm as a call of its own: the sweeps then get a register
 // allocation of their own instead of sharing it with the caller's live state
 // (the pipelined kernel's consumer runs at 192 registers per thread).

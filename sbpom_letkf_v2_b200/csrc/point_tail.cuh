@@ -75,7 +75,9 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
     }
     cta_sync();
     const double tol = jacobi_tol_of(p, k);
-    bits |= jacobi_eig<(KP / 4 < 16 ? KP / 4 : 16)>(Nb, n, ldn, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+    constexpr int ED = KP / 4 < 16 ? KP / 4 : 16;
+    bits |= EIG_CALL ? jacobi_eig_call<ED>(Nb, n, ldn, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw)
+                     : jacobi_eig<ED>(Nb, n, ldn, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
     vt_times(Nb, n, ldn, S.b, S.c);  // c = Lambda^-1 Q^T d
     cta_sync();
     if (tid < n) S.c[tid] /= S.lam[tid];
@@ -88,7 +90,10 @@ __device__ __forceinline__ void point_tail(const sbletkf_params &p, const ObsVie
                        : jacobi_eig_warm<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40,
                                                  S.cw, vprev);
     else
-      bits |= jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40, S.lidx, S.cw);
+      bits |= EIG_CALL ? jacobi_eig_call<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40,
+                                                 S.lidx, S.cw)
+                       : jacobi_eig<KP / 4>(S.u, k, S.ldb, tol, jacobi_stop_of(p), p.max_sweeps, S.lam, S.iws + 40,
+                                            S.lidx, S.cw);
     if (vprev) {  // keep this level's eigenvectors for the next one
       for (int e = tid; e < k * k; e += kThreads) vprev[e] = S.u[(long)(e / k) * S.ldb + (e % k)];
       warm = 1;
