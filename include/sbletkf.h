@@ -101,8 +101,8 @@ typedef struct sbletkf_params {
   double re;           /* earth radius [m]           (:28)                    */
   double pi;           /* (:27)                                               */
   double jacobi_tol;   /* smallest relative rotation the eigensolve applies;
-                          <= 0: k * 2^-52 on the FP64 path, 1e-9 on the mixed
-                          path (three orders under its Gram's error)        */
+                          <= 0: k * 2^-52 on the FP64 path, 1e-8 on the mixed
+                          path (well under its Gram's ~1e-6 error)          */
   double tc_max_cand;  /* mixed path: points whose search box holds more candidates
                           use the FP64 Gram; <= 0: library default 12288   */
   double jacobi_stop;  /* the eigensolve ends after a sweep whose largest relative

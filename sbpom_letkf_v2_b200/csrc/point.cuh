@@ -32,10 +32,10 @@ __host__ __device__ inline double jacobi_stop_of(const sbletkf_params &p) {
   return p.jacobi_stop > 0.0 ? p.jacobi_stop : p.precision == SBLETKF_PREC_MIXED ? kJacobiStopMixed : kJacobiStop;
 }
 // Smallest relative rotation the sweeps apply, unless sbletkf_params.jacobi_tol
-// sets another: k eps on the FP64 path; 1e-9 on the mixed path, where the
-// rotations below it (left as residual) are three orders under the Gram's
-// own error and only cost the last sweep time.
-constexpr double kJacobiTolMixed = 1e-9;
+// sets another: k eps on the FP64 path; 1e-8 on the mixed path, where the
+// rotations below it (left as residual, ~3e-8) are well under the Gram's own
+// ~1e-6 error and only cost the last sweep time.
+constexpr double kJacobiTolMixed = 1e-8;
 __host__ __device__ inline double jacobi_tol_of(const sbletkf_params &p, int k) {
   return p.jacobi_tol > 0.0 ? p.jacobi_tol
          : p.precision == SBLETKF_PREC_MIXED ? kJacobiTolMixed

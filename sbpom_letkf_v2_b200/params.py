@@ -90,7 +90,7 @@ class LETKFParams:
     smax: float = 50.0
     re: float = 6371.3e3            # :28
     pi: float = 4.0 * math.atan(1.0)  # :27
-    jacobi_tol: float = 0.0         # 0 -> library default (k * eps FP64, 1e-9 mixed)
+    jacobi_tol: float = 0.0         # 0 -> library default (k * eps FP64, 1e-8 mixed)
     tc_max_cand: float = 0.0        # mixed path: FP64 Gram above this many box candidates (0 -> 12288)
     jacobi_stop: float = 0.0        # end the eigensolve after a sweep with no relative rotation above this (0 -> 1e-10 FP64, 1e-5 mixed)
 
